@@ -1,0 +1,311 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 APT step on the throughput configuration.
+
+Workload (one GPU): 3D multi-grain directional solidification, line (frozen
+gradient) temperature, 256 x 256 x 512 interior cells, 600 seeded Voronoi grains,
+NUM_PF = 8 slots, FP32 storage, periodic x/y and no-flux z; synthetic seeded
+inputs of the reference's shapes (the reference ships no dataset).
+
+A "step" is one explicit time step of the whole grid (one launch of the fused
+step kernel).  `value` = interior cells x K / device time of K steps (CUDA events
+on the solver's stream, inputs resident in HBM; the 4.4 GB of pair buffers are
+far larger than L2, so no flush is needed).  `e2e` = the same metric through the
+C ABI with host buffers: initial fields host->device, all steps of the
+configuration (2000), argmax map and grain volumes device->host.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cupf|reference]
+Under torchrun each rank runs an independent replica (the step does not shard:
+no collective on the data path); value sums the replicas' cells over the max
+of the ranks' times.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+INTERIOR = (256, 256, 512)
+NUM_PF = 8
+GRAINS = 600
+SEED = 0
+CONFIG_STEPS = 2000
+METRIC = "3D APT Mcell-upd/s"
+UNIT = "Mcell-upd/s"
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "apt_step_c2_ncu.md")
+
+
+def workload_config(extra=None):
+    c = {"workload": "3D APT line step %dx%dx%d interior, NUM_PF=%d, %d grains, FP32 storage"
+                     % (*INTERIOR, NUM_PF, GRAINS),
+         "interior": list(INTERIOR), "num_pf": NUM_PF, "grains": GRAINS, "seed": SEED,
+         "bc": "110", "thermal": "line G=1 K/um R=0.05 m/s", "config_steps": CONFIG_STEPS,
+         "l2": "inputs larger than L2 (2 x 2.2 GB pair buffers), no flush"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join("/tmp", "cupf_clocks_%d_%d.csv" % (os.getpid(), device))
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        load = [v for v in sm if mx and v > 0.3 * max(mx)] or sm
+        return {"sm_mhz": float(np.median(load)) if load else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def measured_peak():
+    try:
+        d = json.load(open(PEAKS))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the step kernel from the committed ncu summary."""
+    try:
+        for line in open(TRAFFIC_PROFILE):
+            if line.startswith("traffic_bytes_per_launch_c2:"):
+                return float(line.split(":")[1])
+    except Exception:
+        pass
+    return None
+
+
+def make_case():
+    from cupf_b200 import cases
+    return cases.line_case(*INTERIOR, num_pf=NUM_PF, num_grains=GRAINS, seed=SEED, bc="110")
+
+
+def cpu_baseline(case, budget_s=15.0, max_steps=4):
+    """FP64 oracle (OpenMP, all host threads) on the same workload: bounded number of steps."""
+    from oracle import CpuOracle
+    o = CpuOracle()
+    ph32, ids = case.initial_slots()
+    ph = ph32.astype(np.float64)
+    ph_b, ids_b = ph.copy(), ids.copy()
+    p = case.params
+    cells = (p.fnx - 2) * (p.fny - 2) * (p.fnz - 2)
+    steps, t_total = 0, 0.0
+    while steps < max_steps and t_total < budget_s:
+        t = float(np.float32(np.float32(steps + 1) * np.float32(p.dt)) * np.float32(p.tau0))
+        t0 = time.perf_counter()
+        o.set_bc(p, ph, ids)
+        o.rhs_psi_f64(case, t, ph, ids, ph_b, ids_b)
+        t_total += time.perf_counter() - t0
+        ph, ph_b = ph_b, ph
+        ids, ids_b = ids_b, ids
+        steps += 1
+    cores = os.cpu_count()
+    return {"value": cells * steps / t_total / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "%d FP64 steps of the full %dx%dx%d grid (%.1f s)" % (steps, *INTERIOR, t_total)}
+
+
+def run_reference(args, ws, rank):
+    """Reference arm: the reference's algorithm on the host cores (the oracle
+    port in double precision, OpenMP), each step a bounded slab of the workload."""
+    if rank != 0:
+        return 0
+    from cupf_b200 import cases
+    from oracle import CpuOracle
+    slab = (INTERIOR[0], INTERIOR[1], 64)
+    c = cases.line_case(*slab, num_pf=NUM_PF, num_grains=GRAINS, seed=SEED, bc="110")
+    o = CpuOracle()
+    ph32, ids = c.initial_slots()
+    ph = ph32.astype(np.float64)
+    ph_b, ids_b = ph.copy(), ids.copy()
+    p = c.params
+    cells = (p.fnx - 2) * (p.fny - 2) * (p.fnz - 2)
+
+    def one(n):
+        nonlocal ph, ph_b, ids, ids_b
+        t = float(np.float32(np.float32(n) * np.float32(p.dt)) * np.float32(p.tau0))
+        o.set_bc(p, ph, ids)
+        o.rhs_psi_f64(c, t, ph, ids, ph_b, ids_b)
+        ph, ph_b = ph_b, ph
+        ids, ids_b = ids_b, ids
+
+    for n in range(args.warmup):
+        one(n + 1)
+    t0 = time.perf_counter()
+    for n in range(args.steps):
+        one(args.warmup + n + 1)
+    dt = time.perf_counter() - t0
+    v = cells * args.steps / dt / 1e6
+    sample = "each step: one FP64 step of a %dx%dx%d slab of the workload" % slab
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": workload_config({"reference_sample": sample}),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="cupf", choices=["cupf", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, ws, rank)
+
+    import torch
+    from cupf_b200.solver import APTSolver
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    device = local if ws > 1 else 0
+    torch.cuda.set_device(device)
+
+    case = make_case()
+    p = case.params
+    cells = (p.fnx - 2) * (p.fny - 2) * (p.fnz - 2)
+    solver = APTSolver(case, device=device)
+    solver.init_from_argmax(case.phi, case.alpha)
+    solver.step(args.warmup)
+    solver.sync()
+
+    def barrier():
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize(device)
+
+    barrier()
+    with ClockSampler(device) as clk:
+        ms = solver.time_steps(args.steps)
+    barrier()
+    if pg:
+        t = torch.tensor([ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    value = ws * cells * args.steps / (ms / 1e3) / 1e6
+
+    # roofline of the step kernel (the only kernel in the timed region)
+    bytes_per_cell = 2 * NUM_PF * 8
+    launch_s = ms / 1e3 / args.steps
+    achieved = cells * bytes_per_cell / launch_s / 1e9
+    peak, peak_kind = measured_peak()
+    traffic = profile_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                "algorithmic_bytes_per_launch": cells * bytes_per_cell}
+
+    # end to end through the C ABI with host buffers: a whole C2 simulation
+    e2e = None
+    if not args.no_e2e:
+        barrier()
+        t0 = time.perf_counter()
+        with APTSolver(case, device=device) as s2:
+            s2.init_from_argmax(case.phi, case.alpha)
+            s2.step(CONFIG_STEPS)
+            phi, alpha = s2.collect(clear=True)
+            vols = s2.grain_volumes(GRAINS)
+        torch.cuda.synchronize(device)
+        e2e_s = time.perf_counter() - t0
+        if pg:
+            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        L = case.length
+        e2e = {"value": ws * cells * CONFIG_STEPS / e2e_s / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": (8 * L) / CONFIG_STEPS,
+               "d2h_bytes_per_step": (8 * L + 8 * (GRAINS + 1)) / CONFIG_STEPS,
+               "steps": CONFIG_STEPS, "seconds": e2e_s,
+               "includes": "handle create + H2D phi/alpha + 2000 steps + argmax D2H + volumes"}
+        assert vols.sum() == cells
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(case)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+                "config": workload_config({"parallelism": "replicas x%d" % ws}),
+                "hbm_gbs": achieved, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "clocks": clk.summary(), "gpu_launches": args.steps,
+                "baseline_metric": "3D APT Mcell-upd/s & HBM GB/s, mixed vs FP32; served sims/hr,"
+                                   " p50/p99 at <=1e-3 err"}
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

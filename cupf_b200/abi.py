@@ -1,0 +1,103 @@
+"""ctypes mirror of include/cupf.h and the loader of the CUDA library.
+
+The library (cupf_b200/libcupf.so) is built in-tree by cupf_b200/build.py.
+Loading fails loudly when it is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcupf.so")
+
+CUPF_MAX_PF = 16
+
+
+class cupf_apt_params(C.Structure):
+    _fields_ = [
+        ("fnx", C.c_int32), ("fny", C.c_int32), ("fnz", C.c_int32),
+        ("num_pf", C.c_int32), ("num_theta", C.c_int32),
+        ("bcX", C.c_int32), ("bcY", C.c_int32), ("bcZ", C.c_int32),
+        ("thermalType", C.c_int32),
+        ("Nx", C.c_int32), ("Ny", C.c_int32), ("Nz", C.c_int32), ("Nt", C.c_int32),
+        ("kin_delta", C.c_float), ("eps", C.c_float), ("G", C.c_float), ("z0", C.c_float),
+        ("underCoolingRate", C.c_float), ("underCoolingRate0", C.c_float), ("L_cp", C.c_float),
+        ("hi", C.c_float), ("lamd", C.c_float), ("dt", C.c_float), ("tau0", C.c_float),
+        ("lyd", C.c_float), ("lzd", C.c_float),
+        ("r0", C.c_float), ("x0", C.c_float), ("angle", C.c_float), ("V", C.c_float),
+        ("mp_len", C.c_float), ("order", C.c_float),
+        ("dx", C.c_float), ("W0", C.c_float),
+        ("undcool_mean", C.c_float), ("undcool_std", C.c_float), ("nuc_Nmax", C.c_float),
+        ("nuc_Nmax0", C.c_float), ("nuc_rad", C.c_float), ("sqrt2", C.c_float),
+        ("pts_cell", C.c_int32), ("seed", C.c_int32), ("haloWidth", C.c_int32),
+        ("reserved", C.c_int32 * 5),
+    ]
+
+
+FP = C.POINTER(C.c_float)
+
+
+class cupf_apt_inputs(C.Structure):
+    _fields_ = [(n, FP) for n in ("x", "y", "z", "sint", "cost", "X_mac", "Y_mac", "Z_mac",
+                                  "t_mac", "psi_mac", "T_3D")]
+
+
+STATUS = {0: "CUPF_OK", 1: "CUPF_ERR_INVALID", 2: "CUPF_ERR_CUDA", 3: "CUPF_ERR_OOM",
+          4: "CUPF_ERR_UNSUPPORTED", 5: "CUPF_ERR_TIMEOUT", 6: "CUPF_ERR_IO", 7: "CUPF_ERR_STATE"}
+
+PREC = {"fp32": 0, "bf16": 1, "fp16": 2}
+
+
+class CupfError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s: %s" % (STATUS.get(status, status), msg))
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    """Load libcupf.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libcupf.so not built (run cupf_b200/build.py): %s" % LIB_PATH)
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        L.cupf_last_error.restype = C.c_char_p
+        L.cupf_abi_version.restype = C.c_int
+        L.cupf_struct_size.argtypes = [C.c_int]
+        L.cupf_struct_size.restype = C.c_size_t
+        for name, args in {
+            "cupf_apt_create": [C.POINTER(cupf_apt_params), C.POINTER(cupf_apt_inputs), C.c_int,
+                                C.c_int, C.POINTER(vp)],
+            "cupf_apt_destroy": [vp],
+            "cupf_apt_init_from_argmax": [vp, FP, C.POINTER(C.c_int32)],
+            "cupf_apt_set_slots": [vp, FP, C.POINTER(C.c_int32), C.c_int64],
+            "cupf_apt_get_slots": [vp, FP, C.POINTER(C.c_int32)],
+            "cupf_apt_step": [vp, C.c_int32, C.c_int32],
+            "cupf_apt_steps_done": [vp, C.POINTER(C.c_int64)],
+            "cupf_apt_collect": [vp, C.c_int32, FP, C.POINTER(C.c_int32)],
+            "cupf_apt_grain_volumes": [vp, C.c_int32, C.POINTER(C.c_int64)],
+            "cupf_apt_move_domain": [vp, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_int32)],
+            "cupf_apt_get_archive": [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)],
+            "cupf_apt_get_z": [vp, FP],
+            "cupf_apt_sync": [vp, C.c_int32],
+            "cupf_apt_time_steps": [vp, C.c_int32, FP],
+        }.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        L.cupf_apt_stream.argtypes = [vp]
+        L.cupf_apt_stream.restype = vp
+        _lib = L
+    return _lib
+
+
+def check(status):
+    if status != 0:
+        raise CupfError(status, lib().cupf_last_error().decode())
+    return status

@@ -1,0 +1,57 @@
+// apt_common.cuh — shared device definitions of the B200 APT step.
+//
+// Device memory layout of one slot buffer ("pair planes"):
+//   pair[slot][z][y][x]   with x pitch xp (even, >= fnx), 8-byte pairs
+//   pair = { float phi, int32 id }           (id -1 = empty slot)
+// i.e. the reference's SoA slot layout (devicefunc.cu_inl:24-29) with phi and
+// id interleaved and the x rows padded so every row starts on a 16-byte
+// boundary, which is what a TMA tensor map needs.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/cupf.h"
+
+namespace cupf {
+
+constexpr double LS = -0.995;     // liquid threshold (APTPhaseField.cu:25)
+constexpr double ID_DROP = -0.9999; // id is dropped below this phi (:341)
+
+// Per-launch arguments of the step kernel (passed by value).
+struct StepArgs {
+  int fnx, fny, fnz, xp;
+  long long slot_stride;  // pairs per slot plane set = xp*fny*fnz
+  int bcX, bcY, bcZ;
+  int ntx, nty, nzc, zc;  // tile grid and z-chunk length
+  int num_theta, thermalType, use_iuc;
+  float t;
+  float kin_delta, eps, G, z0, uc, uc0, L_cp, hi, lamd, dt;
+  float lyd, lzd, r0, x0, angle, V, mp_len, order;
+  int Nx, Ny, Nz;
+  const float* x;
+  const float* y;
+  const float* z;
+  const float* sint;
+  const float* cost;
+  const float* X_mac;
+  const float* Y_mac;
+  const float* Z_mac;
+  const float* psi_mac;
+  const uint2* in;   // pair buffer read this step
+  uint2* out;        // pair buffer written this step
+  int* err;          // device error word (0 = ok)
+};
+
+// Boundary map of one coordinate (APTsetBC3D, APTPhaseField.cu:111-112,134-135,157-158):
+// no-flux mirrors about the first/last interior point, periodic wraps.
+__host__ __device__ __forceinline__ int bc_map(int c, int fn, int bc) {
+  if (c == 0) return bc == 0 ? 2 : fn - 2;
+  if (c == fn - 1) return bc == 0 ? fn - 3 : 1;
+  return c;
+}
+
+enum ErrCode { ERR_TMA_TIMEOUT = 1 };
+
+}  // namespace cupf

@@ -1,0 +1,332 @@
+// apt_step.cuh — the fused APT step kernel for sm_100a.
+//
+// One launch = one explicit step of the reference's APTsetBC3D + APTrhs_psi
+// pair (3DgrainMPI/APTPhaseField.cu:93-174, 178-354): boundary fill, neighbour
+// grain-id gather with the first-seen merge, per-slot anisotropic update.
+//
+// Work decomposition: a CTA owns a TX x TY column tile of interior (x, y) cells
+// and a z chunk of ZC planes; one thread per (x, y) column marches z.  Planes of
+// the input pair buffer (all NUM_PF slots, tile plus one-cell halo) stream into
+// shared memory through a ring of S stages filled by TMA
+// (cp.async.bulk.tensor.4d, one 4-D box {TX+2, TY+2, 1, NP} per plane) and
+// completed on per-stage mbarriers.  Computing plane k needs planes k-1, k, k+1
+// resident; planes k+2, k+3 are in flight.
+//
+// Boundary fill is done on the read side: plane indices 0 and fnz-1 are loaded
+// from their mapped source planes, and halo cells of x/y are overwritten in
+// shared memory from their mapped interior source in global memory.  The halo
+// cells of the pair buffers in HBM are therefore never written by the step; a
+// separate fill kernel materialises them before any read-back.
+//
+// After a plane lands, each cell of its tile gets a slot-occupancy bit mask
+// (bit p set when slot p holds an id).  The merge then visits only occupied
+// slots of the 7 stencil points, in the reference's order (D,B,L,C,R,T,U) x
+// slot, and records for every stencil point which source slot feeds which
+// output slot (4-bit codes), so the per-slot update reads exactly the values
+// the reference's local_phs array would hold, including its aliasing write on
+// merge overflow (local_phs[s][NUM_PF] == local_phs[s+1][0]).
+#pragma once
+
+#include "apt_update.cuh"
+
+namespace cupf {
+
+constexpr int TX = 32;
+constexpr int TY = 8;
+constexpr int NTHREADS = TX * TY;
+constexpr int BW = TX + 2;  // box width (cells)
+constexpr int BH = TY + 2;  // box height
+constexpr int BCELLS = BW * BH;
+constexpr int STAGES = 5;
+
+template <int NP>
+struct StepSmem {
+  static constexpr int kBoxBytes = NP * BCELLS * 8;                // bytes one TMA plane load delivers
+  static constexpr int kStageBytes = (kBoxBytes + 127) & ~127;  // stage stride (TMA dst: 128 B aligned)
+  static constexpr int kStagePairs = kStageBytes / 8;
+  static constexpr int kMaskOff = STAGES * kStageBytes;
+  static constexpr int kBarOff = (kMaskOff + STAGES * BCELLS * 2 + 7) & ~7;
+  static constexpr int kBytes = kBarOff + STAGES * 8 + 16;  // + abort word, issued count
+};
+
+template <int NP>
+using CodeMap = typename std::conditional<(NP <= 8), uint32_t, unsigned long long>::type;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Wait for a stage with a bounded spin: about one second of SM clock, then
+// give up and report (the caller records an error and carries on so that every
+// thread still reaches every barrier).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > (1ll << 31)) return false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ void tma_load_plane(void* dst, const CUtensorMap* map, uint64_t* bar,
+                                               int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(0), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+template <int NP>
+__global__ void __launch_bounds__(NTHREADS, 2)
+    apt_step_kernel(const __grid_constant__ CUtensorMap tmap, const StepArgs a) {
+  using Map = CodeMap<NP>;
+  using Smem = StepSmem<NP>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint2* stages = reinterpret_cast<uint2*>(smem);
+  uint16_t* masks = reinterpret_cast<uint16_t*>(smem + Smem::kMaskOff);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Smem::kBarOff);
+  int* s_abort = reinterpret_cast<int*>(smem + Smem::kBarOff + STAGES * 8);  // first failed plane + 1
+  int* s_issued = s_abort + 1;  // planes issued so far (written by thread 0)
+
+  const int tid = threadIdx.x;
+  const int tx = tid % TX, ty = tid / TX;
+  int b = blockIdx.x;
+  const int zci = b % a.nzc;
+  b /= a.nzc;
+  const int txi = b % a.ntx;
+  const int tyi = b / a.ntx;
+  const int x0 = 1 + TX * txi;  // first interior x of the tile
+  const int y0 = 1 + TY * tyi;
+  const int k_begin = 1 + a.zc * zci;
+  const int k_end = min(k_begin + a.zc, a.fnz - 1);
+  const int nplanes = k_end - k_begin + 2;  // planes k_begin-1 .. k_end
+  const long long ss = a.slot_stride;
+  const long long plane_pairs = (long long)a.xp * a.fny;
+
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
+    *s_abort = 0;
+    *s_issued = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  auto issue = [&](int q) {  // plane index q -> logical z = k_begin - 1 + q
+    const int s = q % STAGES;
+    const int zl = k_begin - 1 + q;
+    const int zp = bc_map(zl, a.fnz, a.bcZ);
+    mbar_arrive_expect_tx(&bars[s], Smem::kBoxBytes);
+    tma_load_plane(stages + (size_t)s * Smem::kStagePairs, &tmap, &bars[s], x0 - 1, y0 - 1, zp);
+    *s_issued = q + 1;
+  };
+
+  if (tid == 0) {
+    const int npre = min(STAGES, nplanes);
+    for (int q = 0; q < npre; ++q) issue(q);
+  }
+
+  // Wait for plane q, patch its x/y halo cells from their mapped sources, and
+  // compute the occupancy masks of its cells (same thread per cell for both).
+  auto land = [&](int q) {
+    const int s = q % STAGES;
+    const uint32_t parity = (uint32_t)((q / STAGES) & 1);
+    if (!*s_abort) {
+      if (!mbar_wait_bounded(&bars[s], parity)) {
+        atomicCAS(s_abort, 0, q + 1);
+        atomicExch(a.err, ERR_TMA_TIMEOUT);
+      }
+    }
+    uint2* st = stages + (size_t)s * Smem::kStagePairs;
+    const int zl = k_begin - 1 + q;
+    const int zp = bc_map(zl, a.fnz, a.bcZ);
+    for (int c = tid; c < BCELLS; c += NTHREADS) {
+      const int sx = c % BW, sy = c / BW;
+      const int gx = x0 - 1 + sx, gy = y0 - 1 + sy;
+      const bool inside = gx < a.fnx && gy < a.fny;
+      if (inside && (gx == 0 || gx == a.fnx - 1 || gy == 0 || gy == a.fny - 1)) {
+        const int mx = bc_map(gx, a.fnx, a.bcX), my = bc_map(gy, a.fny, a.bcY);
+        const long long src = (long long)zp * plane_pairs + (long long)my * a.xp + mx;
+#pragma unroll
+        for (int p = 0; p < NP; ++p) st[p * BCELLS + c] = __ldg(a.in + p * ss + src);
+      }
+      uint32_t m = 0;
+#pragma unroll
+      for (int p = 0; p < NP; ++p) m |= (uint32_t)((int)st[p * BCELLS + c].y != -1) << p;
+      masks[s * BCELLS + c] = (uint16_t)m;
+    }
+  };
+
+  land(0);
+  land(1);
+
+  const int gx = x0 + tx, gy = y0 + ty;
+  const bool valid = gx <= a.fnx - 2 && gy <= a.fny - 2;
+  const int c = (ty + 1) * BW + (tx + 1);
+
+  for (int k = k_begin; k < k_end; ++k) {
+    const int qk = k - k_begin + 1;
+    land(qk + 1);
+    __syncthreads();
+    if (tid == 0 && qk >= 2 && qk - 2 + STAGES < nplanes && !*s_abort) {
+      fence_proxy_async();
+      issue(qk - 2 + STAGES);
+    }
+    if (!valid) continue;
+
+    const int sD = (qk - 1) % STAGES, sC = qk % STAGES, sU = (qk + 1) % STAGES;
+    const uint2* pD = stages + (size_t)sD * Smem::kStagePairs + c;
+    const uint2* pC = stages + (size_t)sC * Smem::kStagePairs + c;
+    const uint2* pU = stages + (size_t)sU * Smem::kStagePairs + c;
+    const uint2* pts[7] = {pD, pC - BW, pC - 1, pC, pC + 1, pC + BW, pU};
+    uint32_t mk[7];
+    mk[0] = masks[sD * BCELLS + c];
+    mk[1] = masks[sC * BCELLS + c - BW];
+    mk[2] = masks[sC * BCELLS + c - 1];
+    mk[3] = masks[sC * BCELLS + c];
+    mk[4] = masks[sC * BCELLS + c + 1];
+    mk[5] = masks[sC * BCELLS + c + BW];
+    mk[6] = masks[sU * BCELLS + c];
+
+    uint2* outp = a.out + (long long)k * plane_pairs + (long long)gy * a.xp + gx;
+    const uint32_t any = mk[0] | mk[1] | mk[2] | mk[3] | mk[4] | mk[5] | mk[6];
+    if (any == 0) {
+      const uint2 empty = make_uint2(__float_as_uint(-1.0f), 0xFFFFFFFFu);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) outp[p * ss] = empty;
+      continue;
+    }
+
+    // ---- merge: first-seen order over (D,B,L,C,R,T,U) x slot
+    int L[NP];
+#pragma unroll
+    for (int q = 0; q < NP; ++q) L[q] = -1;
+    int n = 0;
+    Map code[7];
+    float alias[7];
+#pragma unroll
+    for (int s = 0; s < 7; ++s) {
+      code[s] = ~(Map)0;
+      alias[s] = -1.0f;
+    }
+#pragma unroll
+    for (int s = 0; s < 7; ++s) {
+      uint32_t m = mk[s];
+      while (m) {
+        const int p = __ffs(m) - 1;
+        m &= m - 1;
+        const uint2 pr = pts[s][p * BCELLS];
+        const int id = (int)pr.y;
+        int j = n;
+#pragma unroll
+        for (int q = NP - 1; q >= 0; --q)
+          if (L[q] == id) j = q;
+        if (j == n) {
+          if (n < NP) {
+#pragma unroll
+            for (int q = 0; q < NP; ++q)
+              if (q == n) L[q] = id;
+            ++n;
+          } else {
+            // local_phs[s][NUM_PF] aliases local_phs[s+1][0]; past the array at s == 6
+            if (s < 6) {
+              code[s + 1] = (code[s + 1] & ~(Map)0xF) | (Map)0xE;
+              alias[s + 1] = __uint_as_float(pr.x);
+            }
+            continue;
+          }
+        }
+        const int sh = 4 * j;
+        code[s] = (code[s] & ~((Map)0xF << sh)) | ((Map)p << sh);
+      }
+    }
+
+    auto fetch = [&](int s, int j) -> float {
+      const uint32_t cd = (uint32_t)(code[s] >> (4 * j)) & 0xF;
+      if (cd == 0xF) return -1.0f;
+      if (cd == 0xE) return alias[s];
+      return __uint_as_float(pts[s][cd * BCELLS].x);
+    };
+
+    // center values of every slot (for the repulsion sum)
+    float phc[NP];
+#pragma unroll
+    for (int q = 0; q < NP; ++q) phc[q] = (q < n) ? fetch(3, q) : -1.0f;
+
+    float Up = 0.0f;
+    bool upd = true;
+    {
+      float T;
+      upd = tinterp(a, gx, gy, k, &T);
+      Up = __fdiv_rn(T, a.L_cp);
+    }
+
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+      uint2 o;
+      if (j >= n) {
+        o = make_uint2(__float_as_uint(-1.0f), 0xFFFFFFFFu);
+      } else if (!upd) {
+        o = outp[j * ss];  // reference leaves the slot unwritten
+      } else {
+        float ph7[7];
+#pragma unroll
+        for (int s = 0; s < 7; ++s) ph7[s] = fetch(s, j);
+        const int id = L[j];
+        float sina = 0.0f, cosa = 1.0f, sinb = 0.0f, cosb = 1.0f;
+        // ids are >= 0 here (cupf_apt_set_slots rejects other negative ids); the
+        // bound check only keeps a corrupted id from reading outside the tables
+        const int tid2 = id <= a.num_theta ? id : (id % a.num_theta) + 1;
+        if ((double)ph7[3] > LS && (unsigned)tid2 <= (unsigned)a.num_theta) {
+          sina = __ldg(a.sint + tid2);
+          cosa = __ldg(a.cost + tid2);
+          sinb = __ldg(a.sint + tid2 + a.num_theta);
+          cosb = __ldg(a.cost + tid2 + a.num_theta);
+        }
+        float repul = 0.0f;
+#pragma unroll
+        for (int q = 0; q < NP; ++q)
+          if (q != j && q < n) repul = repul_add(repul, phc[q]);
+        const float nv = slot_update(a, ph7, sina, cosa, sinb, cosb, repul, Up);
+        o = make_uint2(__float_as_uint(nv), ((double)nv < ID_DROP) ? 0xFFFFFFFFu : (uint32_t)id);
+      }
+      outp[j * ss] = o;
+    }
+  }
+
+  // After a timed-out wait no further loads were issued; before the CTA exits
+  // (and its shared memory is reused) wait, again bounded, for those in flight.
+  __syncthreads();
+  if (tid == 0 && *s_abort) {
+    for (int q = *s_abort - 1; q < *s_issued; ++q)
+      mbar_wait_bounded(&bars[q % STAGES], (uint32_t)((q / STAGES) & 1));
+  }
+}
+
+}  // namespace cupf

@@ -1,0 +1,167 @@
+// apt_update.cuh — per-slot explicit update of the APT step (single precision).
+//
+// Restates the arithmetic of APTrhs_psi (3DgrainMPI/APTPhaseField.cu:254-348),
+// kine_ani (:36-52) and the thermal models (:278-327, devicefunc.cu_inl:85-125).
+// Every operation is written with an explicit rounding intrinsic, so nvcc
+// cannot fuse anything on its own: the sites where the reference's build fuses
+// a product into a sum (nvcc's default -fmad=true) are chosen by the Contract
+// constants below, which are pinned bit-for-bit against the reference kernels
+// compiled for sm_100a.  Site order and meaning match oracle/apt_oracle.c.
+#pragma once
+
+#include "apt_common.cuh"
+
+namespace cupf {
+
+struct Contract {
+  // 0 = separate multiply and add, 1 = fuse the left product, 2 = fuse the right one.
+  // Pinned: with these choices every step of the reference kernels recorded on a
+  // B200 is reproduced bit for bit (AS and TD are indistinguishable on those
+  // inputs and keep the compiler's usual left fusion).
+  static constexpr int AS = 1, UX_IN = 1, UX_OUT = 1, UY = 2, UZ_IN = 1, UZ_OUT = 1,
+                       MAG_IN = 0, MAG_OUT = 0, Q_IN = 2, Q_OUT = 1, DIFF = 1, REP = 1, W = 1,
+                       E1 = 2, INNER = 1, RHS = 1, NEW = 1, TD = 1;
+};
+
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float ffma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
+// x*y + u*v under contraction mode M
+template <int M>
+__device__ __forceinline__ float sop(float x, float y, float u, float v) {
+  if (M == 1) return ffma(x, y, fmul(u, v));
+  if (M == 2) return ffma(u, v, fmul(x, y));
+  return fadd(fmul(x, y), fmul(u, v));
+}
+
+// 4-fold kinetic anisotropy of the rotated normal (APTPhaseField.cu:36-52).
+__device__ __forceinline__ float kine_ani(float ux, float uy, float uz, float cosa, float sina,
+                                          float cosb, float sinb, float kd, float eps) {
+  using K = Contract;
+  float a_s = K::AS ? ffma(3.0f, kd, 1.0f) : fadd(1.0f, fmul(3.0f, kd));
+  float epsilon = __fdiv_rn(fmul(-4.0f, kd), a_s);
+  float s = sop<K::UX_IN>(fmul(cosa, cosb), ux, fmul(sina, cosb), uy);
+  float rx = K::UX_OUT ? ffma(-sinb, uz, s) : fsub(s, fmul(sinb, uz));
+  float ry = fadd(sop<K::UY>(-sina, ux, cosa, uy), 0.0f);
+  s = sop<K::UZ_IN>(fmul(cosa, sinb), ux, fmul(sina, sinb), uy);
+  float rz = K::UZ_OUT ? ffma(cosb, uz, s) : fadd(s, fmul(cosb, uz));
+  float ux2 = fmul(rx, rx), uy2 = fmul(ry, ry), uz2 = fmul(rz, rz);
+  float mag = sop<K::MAG_IN>(rx, rx, ry, ry);
+  mag = K::MAG_OUT ? ffma(rz, rz, mag) : fadd(mag, uz2);
+  float mag2 = fmul(mag, mag);
+  if (mag > eps) {
+    float q = sop<K::Q_IN>(ux2, ux2, uy2, uy2);
+    q = K::Q_OUT ? ffma(uz2, uz2, q) : fadd(q, fmul(uz2, uz2));
+    return fmul(a_s, fadd(1.0f, __fdiv_rn(fmul(epsilon, q), mag2)));
+  }
+  return 1.0f;
+}
+
+// interp3Dtemperature (devicefunc.cu_inl:85-125).
+__device__ __forceinline__ float interp3d(const float* __restrict__ u, float x, float y, float z,
+                                          int Nx, int Ny, int Nz, float Dx) {
+  int kx = (int)__fdiv_rn(x, Dx), ky = (int)__fdiv_rn(y, Dx), kz = (int)__fdiv_rn(z, Dx);
+  float dx = fsub(__fdiv_rn(x, Dx), (float)kx);
+  float dy = fsub(__fdiv_rn(y, Dx), (float)ky);
+  float dz = fsub(__fdiv_rn(z, Dx), (float)kz);
+  if (kx == Nx - 1) { kx = Nx - 2; dx = 1.0f; }
+  if (ky == Ny - 1) { ky = Ny - 2; dy = 1.0f; }
+  if (kz == Nz - 1) { kz = Nz - 2; dz = 1.0f; }
+  long long o = kx + (long long)ky * Nx + (long long)kz * Nx * Ny;
+  long long on = kx + (long long)ky * Nx + (long long)(kz + 1) * Nx * Ny;
+  float a = fmul(fsub(1.0f, dx), fsub(1.0f, dy)), b = fmul(fsub(1.0f, dx), dy);
+  float c = fmul(dx, fsub(1.0f, dy)), d = fmul(dx, dy);
+  float p0 = ffma(c, __ldg(u + o + 1), ffma(a, __ldg(u + o), fmul(b, __ldg(u + o + Nx))));
+  p0 = ffma(d, __ldg(u + o + Nx + 1), p0);
+  float p1 = ffma(c, __ldg(u + on + 1), ffma(a, __ldg(u + on), fmul(b, __ldg(u + on + Nx))));
+  p1 = ffma(d, __ldg(u + on + Nx + 1), p1);
+  return ffma(p0, fsub(1.0f, dz), fmul(p1, dz));
+}
+
+// Undercooling at (i,j,k) and time t (APTPhaseField.cu:278-327).  Returns false
+// where the reference skips the update (`continue`: the slot keeps what the
+// output buffer already holds).
+__device__ __forceinline__ bool tinterp(const StepArgs& a, int i, int j, int k, float* T) {
+  const float t = a.t;
+  if (a.use_iuc) {
+    *T = __double2float_rn(__dmul_rn(__dmul_rn((double)(-a.uc0), 1e6), (double)t));
+    return true;
+  }
+  if (a.thermalType == 1) {
+    float g = fmul(a.G, fsub(__ldg(a.z + k), a.z0));
+    double m = __dmul_rn((double)a.uc, 1e6);
+    double r = Contract::TD ? __fma_rn(-m, (double)t, (double)g)
+                            : __dsub_rn((double)g, __dmul_rn(m, (double)t));
+    *T = __double2float_rn(r);
+    return true;
+  }
+  if (a.thermalType == 2) {
+    float u = fsub(__ldg(a.y + j), fmul(0.5f, a.lyd));
+    float v = fsub(fsub(__ldg(a.z + k), a.z0), a.lzd);
+    float dist = fsub(__fsqrt_rn(ffma(u, u, fmul(v, v))), a.r0);
+    double m = __dmul_rn((double)a.uc, 1e6);
+    *T = __double2float_rn(__fma_rn(-m, (double)t, (double)fmul(-a.G, dist)));
+    return true;
+  }
+  if (a.thermalType == 3) {
+    float lm = __fdiv_rn(fsub(a.r0, a.z0), tanf(a.angle));
+    float xl = fsub(__ldg(a.x + i), 0.0f);
+    float r0x = fadd(a.z0, __fdiv_rn(fmul(fsub(a.r0, a.z0), xl), lm));
+    float u = fsub(__ldg(a.y + j), fmul(0.5f, a.lyd));
+    float zt = fsub(fadd(a.z0, a.lzd), __ldg(a.z + k));
+    float dist = fmul(cosf(a.angle), fsub(__fsqrt_rn(ffma(u, u, fmul(zt, zt))), r0x));
+    if ((double)xl > __fma_rn((double)fmul(a.V, t), 1e6, (double)lm)) return false;
+    double m = __dmul_rn((double)a.uc, 1e6);
+    *T = __double2float_rn(__fma_rn(-m, (double)t, (double)fmul(-a.G, dist)));
+    return true;
+  }
+  if (a.thermalType == 4) {
+    float xq = __double2float_rn(
+        __dsub_rn((double)__ldg(a.x + i), __dmul_rn((double)fmul(a.V, t), 1e6)));
+    if (xq > fadd(a.mp_len, a.x0) || xq < 0.0f) return false;
+    float Dx = fsub(__ldg(a.X_mac + 1), __ldg(a.X_mac));
+    float v = interp3d(a.psi_mac, fsub(xq, __ldg(a.X_mac)), fsub(__ldg(a.y + j), __ldg(a.Y_mac)),
+                       fsub(__ldg(a.z + k), __ldg(a.Z_mac)), a.Nx, a.Ny, a.Nz, Dx);
+    *T = (a.order == 100.0f) ? -v : fmul(-a.G, v);
+    return true;
+  }
+  *T = 0.0f;
+  return true;
+}
+
+// New phi of one active slot (APTPhaseField.cu:254-340).  ph[0..6] are the
+// slot's values at D,B,L,C,R,T,U; repul the repulsion sum; Up = T/L_cp.
+__device__ __forceinline__ float slot_update(const StepArgs& a, const float ph[7], float sina,
+                                             float cosa, float sinb, float cosb, float repul,
+                                             float Up) {
+  using K = Contract;
+  const float phD = ph[0], phB = ph[1], phL = ph[2], phC = ph[3], phR = ph[4], phT = ph[5],
+              phU = ph[6];
+  float phx = fmul(fsub(phR, phL), 0.5f);
+  float phy = fmul(fsub(phT, phB), 0.5f);
+  float phz = fmul(fsub(phU, phD), 0.5f);
+  float A2 = kine_ani(phx, phy, phz, cosa, sina, cosb, sinb, a.kin_delta, a.eps);
+  float sum = fadd(fadd(fadd(fadd(fadd(phR, phL), phT), phB), phU), phD);
+  float diff = K::DIFF ? ffma(-6.0f, phC, sum) : fsub(sum, fmul(6.0f, phC));
+  float w = K::W ? ffma(-phC, phC, 1.0f) : fsub(1.0f, fmul(phC, phC));
+  float dh = fmul(diff, a.hi);
+  float E1 = sop<K::E1>(dh, a.hi, w, phC);
+  float m6 = fmul(6.0f, fadd(phC, 1.0f));
+  float inner;
+  if (K::INNER == 1) inner = ffma(w, w, -fmul(m6, repul));
+  else if (K::INNER == 2) inner = ffma(-m6, repul, fmul(w, w));
+  else inner = fsub(fmul(w, w), fmul(m6, repul));
+  float lu = fmul(a.lamd, Up);
+  float rhs = K::RHS ? ffma(-lu, inner, E1) : fsub(E1, fmul(lu, inner));
+  float dphi = __fdiv_rn(rhs, A2);
+  return K::NEW ? ffma(a.dt, dphi, phC) : fadd(phC, fmul(a.dt, dphi));
+}
+
+__device__ __forceinline__ float repul_add(float repul, float phc) {
+  float q = fadd(phc, 1.0f);
+  return Contract::REP ? ffma(fmul(0.25f, q), q, repul) : fadd(repul, fmul(fmul(0.25f, q), q));
+}
+
+}  // namespace cupf

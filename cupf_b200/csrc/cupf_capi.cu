@@ -1,0 +1,633 @@
+// cupf_capi.cu — C ABI of the B200 APT solver (include/cupf.h).
+//
+// Owns the device state of one simulation: two pair-plane buffers (ping-pong),
+// their TMA tensor maps, coordinates / orientation tables, the argmax fields,
+// the moving-domain archive and one CUDA stream.  Every call checks every CUDA
+// return code and maps failures to a cupf_status with a per-thread message.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/cupf.h"
+#include "apt_aux.cuh"
+#include "apt_step.cuh"
+
+using namespace cupf;
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_err;
+
+static cupf_status fail(cupf_status st, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return st;
+}
+
+#define CK(call)                                                                       \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return fail(e_ == cudaErrorMemoryAllocation ? CUPF_ERR_OOM : CUPF_ERR_CUDA,      \
+                  "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__,   \
+                  __LINE__);                                                           \
+  } while (0)
+
+extern "C" const char* cupf_last_error(void) { return g_err.c_str(); }
+extern "C" int cupf_abi_version(void) { return CUPF_ABI_VERSION; }
+extern "C" size_t cupf_struct_size(int which) {
+  return which == 0 ? sizeof(cupf_apt_params) : which == 1 ? sizeof(cupf_apt_inputs) : 0;
+}
+
+// ------------------------------------------------------------------ tensor maps
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn get_encode() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+// ------------------------------------------------------------------ handle
+struct cupf_apt_handle {
+  cupf_apt_params p;
+  int device = 0;
+  cupf_precision prec = CUPF_PREC_FP32;
+  Grid g;
+  uint2* buf[2] = {nullptr, nullptr};
+  CUtensorMap tmap[2];
+  int cur = 0;  // buffer holding the current state
+  int64_t steps_done = 0;
+  bool initialised = false;
+  cudaStream_t stream = nullptr;
+  // device inputs
+  float *x = nullptr, *y = nullptr, *z = nullptr, *sint = nullptr, *cost = nullptr;
+  float *X_mac = nullptr, *Y_mac = nullptr, *Z_mac = nullptr, *t_mac = nullptr;
+  float *psi_mac = nullptr, *T_3D = nullptr;
+  std::vector<float> z_host;
+  // argmax fields (reference layout, length)
+  float* phi_m = nullptr;
+  int* alpha_m = nullptr;
+  int* err = nullptr;
+  // read-back scratch (reference layout, num_pf * length), allocated on first use
+  float* xfer_ph = nullptr;
+  int* xfer_id = nullptr;
+  // moving domain
+  double* layer_sums = nullptr;
+  int* alpha_full = nullptr;
+  int fnz_f = 0;
+  int* loss_area = nullptr;
+  // reductions
+  unsigned long long* counts = nullptr;
+  long long* first = nullptr;
+  int counts_cap = 0;
+  // launch shape
+  int zc = 64;
+  int ntx = 0, nty = 0, nzc = 0;
+  // events for timing
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+static const char* kOk = "";
+
+static cupf_status upload(float** dst, const float* src, size_t n, cudaStream_t s) {
+  if (n == 0) n = 1;
+  CK(cudaMalloc((void**)dst, n * sizeof(float)));
+  if (src)
+    CK(cudaMemcpyAsync(*dst, src, n * sizeof(float), cudaMemcpyHostToDevice, s));
+  else
+    CK(cudaMemsetAsync(*dst, 0, n * sizeof(float), s));
+  return CUPF_OK;
+}
+
+static cupf_status make_tmap(cupf_apt_handle* h, int b) {
+  EncodeTiledFn enc = get_encode();
+  if (!enc) return fail(CUPF_ERR_CUDA, "cuTensorMapEncodeTiled entry point not available");
+  const Grid& g = h->g;
+  cuuint64_t dims[4] = {(cuuint64_t)g.fnx, (cuuint64_t)g.fny, (cuuint64_t)g.fnz,
+                        (cuuint64_t)g.np};
+  cuuint64_t strides[3] = {(cuuint64_t)g.xp * 8, (cuuint64_t)g.xp * g.fny * 8,
+                           (cuuint64_t)g.ss * 8};
+  cuuint32_t box[4] = {(cuuint32_t)BW, (cuuint32_t)BH, 1u, (cuuint32_t)g.np};
+  cuuint32_t es[4] = {1, 1, 1, 1};
+  CUresult r = enc(&h->tmap[b], CU_TENSOR_MAP_DATA_TYPE_UINT64, 4, h->buf[b], dims, strides, box,
+                   es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(CUPF_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return CUPF_OK;
+}
+
+static void free_handle(cupf_apt_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  void* ptrs[] = {h->buf[0], h->buf[1], h->x, h->y, h->z, h->sint, h->cost, h->X_mac, h->Y_mac,
+                  h->Z_mac, h->t_mac, h->psi_mac, h->T_3D, h->phi_m, h->alpha_m, h->err,
+                  h->xfer_ph, h->xfer_id, h->layer_sums, h->alpha_full, h->loss_area,
+                  h->counts, h->first};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+// ------------------------------------------------------------------ step launch
+template <int NP>
+static cupf_status launch_step_np(cupf_apt_handle* h, const StepArgs& a, const CUtensorMap& m) {
+  static bool configured[64] = {};
+  const int bytes = StepSmem<NP>::kBytes;
+  if (!configured[h->device & 63]) {
+    CK(cudaFuncSetAttribute(apt_step_kernel<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            bytes));
+    configured[h->device & 63] = true;
+  }
+  const int nblk = h->ntx * h->nty * h->nzc;
+  apt_step_kernel<NP><<<nblk, NTHREADS, bytes, h->stream>>>(m, a);
+  CK(cudaGetLastError());
+  return CUPF_OK;
+}
+
+static cupf_status launch_step(cupf_apt_handle* h, const StepArgs& a, const CUtensorMap& m) {
+  switch (h->g.np) {
+#define CASE(N) \
+  case N:       \
+    return launch_step_np<N>(h, a, m);
+    CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8)
+#undef CASE
+    default:
+      return fail(CUPF_ERR_UNSUPPORTED, "num_pf=%d not built (1..8)", h->g.np);
+  }
+}
+
+static StepArgs step_args(cupf_apt_handle* h, float t, int use_iuc) {
+  const cupf_apt_params& p = h->p;
+  StepArgs a;
+  memset(&a, 0, sizeof(a));
+  a.fnx = p.fnx;
+  a.fny = p.fny;
+  a.fnz = p.fnz;
+  a.xp = h->g.xp;
+  a.slot_stride = h->g.ss;
+  a.bcX = p.bcX;
+  a.bcY = p.bcY;
+  a.bcZ = p.bcZ;
+  a.ntx = h->ntx;
+  a.nty = h->nty;
+  a.nzc = h->nzc;
+  a.zc = h->zc;
+  a.num_theta = p.num_theta;
+  a.thermalType = p.thermalType;
+  a.use_iuc = use_iuc;
+  a.t = t;
+  a.kin_delta = p.kin_delta;
+  a.eps = p.eps;
+  a.G = p.G;
+  a.z0 = p.z0;
+  a.uc = p.underCoolingRate;
+  a.uc0 = p.underCoolingRate0;
+  a.L_cp = p.L_cp;
+  a.hi = p.hi;
+  a.lamd = p.lamd;
+  a.dt = p.dt;
+  a.lyd = p.lyd;
+  a.lzd = p.lzd;
+  a.r0 = p.r0;
+  a.x0 = p.x0;
+  a.angle = p.angle;
+  a.V = p.V;
+  a.mp_len = p.mp_len;
+  a.order = p.order;
+  a.Nx = p.Nx;
+  a.Ny = p.Ny;
+  a.Nz = p.Nz;
+  a.x = h->x;
+  a.y = h->y;
+  a.z = h->z;
+  a.sint = h->sint;
+  a.cost = h->cost;
+  a.X_mac = h->X_mac;
+  a.Y_mac = h->Y_mac;
+  a.Z_mac = h->Z_mac;
+  a.psi_mac = h->psi_mac;
+  a.err = h->err;
+  return a;
+}
+
+static void set_zc(cupf_apt_handle* h, int zc) {
+  const int nz = h->p.fnz - 2;
+  h->zc = zc < 1 ? 1 : (zc > nz ? nz : zc);
+  h->ntx = (h->p.fnx - 2 + TX - 1) / TX;
+  h->nty = (h->p.fny - 2 + TY - 1) / TY;
+  h->nzc = (nz + h->zc - 1) / h->zc;
+}
+
+static int grid_for(long long n, int block = 256) {
+  long long b = (n + block - 1) / block;
+  if (b > 148 * 16) b = 148 * 16;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+static cupf_status check_err_word(cupf_apt_handle* h) {
+  int e = 0;
+  CK(cudaMemcpyAsync(&e, h->err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (e != 0) return fail(CUPF_ERR_TIMEOUT, "step kernel reported error %d (TMA wait timed out)", e);
+  return CUPF_OK;
+}
+
+// ------------------------------------------------------------------ API
+extern "C" cupf_status cupf_apt_create(const cupf_apt_params* p, const cupf_apt_inputs* in,
+                                       int device, cupf_precision precision,
+                                       cupf_apt_handle** out) {
+  if (!p || !in || !out) return fail(CUPF_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (p->fnx < 4 || p->fny < 4 || p->fnz < 4)
+    return fail(CUPF_ERR_INVALID, "grid %dx%dx%d too small (each fn >= 4)", p->fnx, p->fny, p->fnz);
+  if ((long long)p->fnx * p->fny * p->fnz > (1ll << 31) - 1)
+    return fail(CUPF_ERR_INVALID, "grid has more than 2^31-1 points");
+  if (p->num_pf < 1 || p->num_pf > 8)
+    return fail(CUPF_ERR_UNSUPPORTED, "num_pf=%d not built (1..8)", p->num_pf);
+  if (p->num_theta < 1) return fail(CUPF_ERR_INVALID, "num_theta must be >= 1");
+  if (p->haloWidth != 1) return fail(CUPF_ERR_INVALID, "haloWidth must be 1");
+  if (p->thermalType < 0 || p->thermalType > 4)
+    return fail(CUPF_ERR_INVALID, "thermalType %d not in 0..4", p->thermalType);
+  if (precision != CUPF_PREC_FP32)
+    return fail(CUPF_ERR_UNSUPPORTED, "precision %d not built", (int)precision);
+  if (!in->x || !in->y || !in->z || !in->sint || !in->cost)
+    return fail(CUPF_ERR_INVALID, "x, y, z, sint and cost are required");
+  if (p->thermalType == 4 && (!in->X_mac || !in->Y_mac || !in->Z_mac || !in->psi_mac))
+    return fail(CUPF_ERR_INVALID, "thermalType 4 needs X_mac, Y_mac, Z_mac and psi_mac");
+
+  cupf_apt_handle* h = new cupf_apt_handle();
+  h->p = *p;
+  h->device = device;
+  h->prec = precision;
+  h->g.fnx = p->fnx;
+  h->g.fny = p->fny;
+  h->g.fnz = p->fnz;
+  h->g.xp = (p->fnx + 1) & ~1;
+  h->g.np = p->num_pf;
+  h->g.ss = (long long)h->g.xp * p->fny * p->fnz;
+  cupf_status st = CUPF_OK;
+#define TRY(x)                  \
+  do {                          \
+    st = (x);                   \
+    if (st != CUPF_OK) {        \
+      free_handle(h);           \
+      return st;                \
+    }                           \
+  } while (0)
+  auto cuda = [&](cudaError_t e, const char* what) -> cupf_status {
+    if (e == cudaSuccess) return CUPF_OK;
+    return fail(e == cudaErrorMemoryAllocation ? CUPF_ERR_OOM : CUPF_ERR_CUDA, "%s: %s", what,
+                cudaGetErrorString(e));
+  };
+  TRY(cuda(cudaSetDevice(device), "cudaSetDevice"));
+  TRY(cuda(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream"));
+  TRY(cuda(cudaEventCreate(&h->ev0), "event"));
+  TRY(cuda(cudaEventCreate(&h->ev1), "event"));
+  const size_t bbytes = (size_t)h->g.ss * h->g.np * sizeof(uint2);
+  for (int b = 0; b < 2; ++b) {
+    TRY(cuda(cudaMalloc((void**)&h->buf[b], bbytes), "slot buffer"));
+    TRY(cuda(cudaMemsetAsync(h->buf[b], 0xFF, bbytes, h->stream), "memset"));
+  }
+  const int nth = 2 * p->num_theta + 1;
+  TRY(upload(&h->x, in->x, p->fnx, h->stream));
+  TRY(upload(&h->y, in->y, p->fny, h->stream));
+  TRY(upload(&h->z, in->z, p->fnz, h->stream));
+  h->z_host.assign(in->z, in->z + p->fnz);
+  TRY(upload(&h->sint, in->sint, nth, h->stream));
+  TRY(upload(&h->cost, in->cost, nth, h->stream));
+  const size_t mNx = p->Nx > 0 ? p->Nx : 1, mNy = p->Ny > 0 ? p->Ny : 1;
+  const size_t mNz = p->Nz > 0 ? p->Nz : 1, mNt = p->Nt > 0 ? p->Nt : 1;
+  TRY(upload(&h->X_mac, in->X_mac, in->X_mac ? mNx : 2, h->stream));
+  TRY(upload(&h->Y_mac, in->Y_mac, in->Y_mac ? mNy : 2, h->stream));
+  TRY(upload(&h->Z_mac, in->Z_mac, in->Z_mac ? mNz : 2, h->stream));
+  TRY(upload(&h->t_mac, in->t_mac, in->t_mac ? mNt : 2, h->stream));
+  TRY(upload(&h->psi_mac, in->psi_mac, in->psi_mac ? mNx * mNy * mNz : 8, h->stream));
+  TRY(upload(&h->T_3D, in->T_3D, in->T_3D ? mNx * mNy * mNz * mNt : 16, h->stream));
+  const size_t L = (size_t)h->g.length();
+  TRY(cuda(cudaMalloc((void**)&h->phi_m, L * sizeof(float)), "phi"));
+  TRY(cuda(cudaMalloc((void**)&h->alpha_m, L * sizeof(int)), "alpha"));
+  TRY(cuda(cudaMemsetAsync(h->phi_m, 0, L * sizeof(float), h->stream), "memset"));
+  TRY(cuda(cudaMemsetAsync(h->alpha_m, 0, L * sizeof(int), h->stream), "memset"));
+  TRY(cuda(cudaMalloc((void**)&h->err, sizeof(int)), "err"));
+  TRY(cuda(cudaMemsetAsync(h->err, 0, sizeof(int), h->stream), "memset"));
+  TRY(cuda(cudaMalloc((void**)&h->layer_sums, p->fnz * sizeof(double)), "layer sums"));
+  for (int b = 0; b < 2; ++b) TRY(make_tmap(h, b));
+  const char* zc_env = getenv("CUPF_ZC");
+  set_zc(h, zc_env ? atoi(zc_env) : 64);
+  TRY(cuda(cudaStreamSynchronize(h->stream), "sync"));
+#undef TRY
+  *out = h;
+  g_err = kOk;
+  return CUPF_OK;
+}
+
+extern "C" cupf_status cupf_apt_destroy(cupf_apt_handle* h) {
+  if (!h) return fail(CUPF_ERR_INVALID, "null handle");
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  free_handle(h);
+  return CUPF_OK;
+}
+
+extern "C" void* cupf_apt_stream(cupf_apt_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+extern "C" cupf_status cupf_apt_init_from_argmax(cupf_apt_handle* h, const float* phi,
+                                                 const int32_t* alpha) {
+  if (!h || !phi || !alpha) return fail(CUPF_ERR_INVALID, "null argument");
+  CK(cudaSetDevice(h->device));
+  const size_t L = (size_t)h->g.length();
+  CK(cudaMemcpyAsync(h->phi_m, phi, L * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->alpha_m, alpha, L * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  init_kernel<<<grid_for(L), 256, 0, h->stream>>>(h->buf[0], h->buf[1], h->phi_m, h->alpha_m,
+                                                   h->g);
+  CK(cudaGetLastError());
+  h->cur = 0;
+  h->steps_done = 0;
+  h->initialised = true;
+  CK(cudaStreamSynchronize(h->stream));
+  return CUPF_OK;
+}
+
+static cupf_status ensure_xfer(cupf_apt_handle* h) {
+  if (!h->xfer_ph) {
+    const size_t n = (size_t)h->g.length() * h->g.np;
+    CK(cudaMalloc((void**)&h->xfer_ph, n * sizeof(float)));
+    CK(cudaMalloc((void**)&h->xfer_id, n * sizeof(int)));
+  }
+  return CUPF_OK;
+}
+
+extern "C" cupf_status cupf_apt_set_slots(cupf_apt_handle* h, const float* ph, const int32_t* ids,
+                                          int64_t steps_done) {
+  if (!h || !ph || !ids) return fail(CUPF_ERR_INVALID, "null argument");
+  CK(cudaSetDevice(h->device));
+  const size_t n = (size_t)h->g.length() * h->g.np;
+  for (size_t i = 0; i < n; ++i)
+    if (ids[i] < -1) return fail(CUPF_ERR_INVALID, "grain id %d at %zu (ids must be >= -1)", ids[i], i);
+  cupf_status st = ensure_xfer(h);
+  if (st) return st;
+  CK(cudaMemcpyAsync(h->xfer_ph, ph, n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->xfer_id, ids, n * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  import_kernel<<<grid_for(n), 256, 0, h->stream>>>(h->buf[0], h->xfer_ph, h->xfer_id, h->g);
+  import_kernel<<<grid_for(n), 256, 0, h->stream>>>(h->buf[1], h->xfer_ph, h->xfer_id, h->g);
+  CK(cudaGetLastError());
+  h->cur = 0;
+  h->steps_done = steps_done;
+  h->initialised = true;
+  CK(cudaStreamSynchronize(h->stream));
+  return CUPF_OK;
+}
+
+static cupf_status fill_halo(cupf_apt_handle* h, int b) {
+  const Grid& g = h->g;
+  const long long n = 2ll * g.fnx * g.fny + 2ll * g.fnx * (g.fnz - 2) + 2ll * (g.fny - 2) * (g.fnz - 2);
+  fill_halo_kernel<<<grid_for(n), 256, 0, h->stream>>>(h->buf[b], g, h->p.bcX, h->p.bcY, h->p.bcZ);
+  CK(cudaGetLastError());
+  return CUPF_OK;
+}
+
+extern "C" cupf_status cupf_apt_get_slots(cupf_apt_handle* h, float* ph, int32_t* ids) {
+  if (!h || !ph || !ids) return fail(CUPF_ERR_INVALID, "null argument");
+  if (!h->initialised) return fail(CUPF_ERR_STATE, "state not initialised");
+  CK(cudaSetDevice(h->device));
+  cupf_status st = ensure_xfer(h);
+  if (st) return st;
+  if ((st = fill_halo(h, h->cur))) return st;
+  const size_t n = (size_t)h->g.length() * h->g.np;
+  export_kernel<<<grid_for(n), 256, 0, h->stream>>>(h->buf[h->cur], h->xfer_ph, h->xfer_id, h->g);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(ph, h->xfer_ph, n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(ids, h->xfer_id, n * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return check_err_word(h);
+}
+
+extern "C" cupf_status cupf_apt_step(cupf_apt_handle* h, int32_t nsteps,
+                                     int32_t use_initial_undercooling) {
+  if (!h) return fail(CUPF_ERR_INVALID, "null handle");
+  if (!h->initialised) return fail(CUPF_ERR_STATE, "step before init");
+  if (nsteps < 0) return fail(CUPF_ERR_INVALID, "nsteps < 0");
+  CK(cudaSetDevice(h->device));
+  for (int n = 0; n < nsteps; ++n) {
+    // t of step m (1-based): (float)m * dt * tau0, as (2*kt+1)*dt*tau0 in evolve
+    const float t = (float)(h->steps_done + 1) * h->p.dt * h->p.tau0;
+    StepArgs a = step_args(h, t, use_initial_undercooling);
+    a.in = h->buf[h->cur];
+    a.out = h->buf[h->cur ^ 1];
+    cupf_status st = launch_step(h, a, h->tmap[h->cur]);
+    if (st) return st;
+    h->cur ^= 1;
+    h->steps_done += 1;
+  }
+  return CUPF_OK;
+}
+
+extern "C" cupf_status cupf_apt_steps_done(cupf_apt_handle* h, int64_t* steps) {
+  if (!h || !steps) return fail(CUPF_ERR_INVALID, "null argument");
+  *steps = h->steps_done;
+  return CUPF_OK;
+}
+
+extern "C" cupf_status cupf_apt_collect(cupf_apt_handle* h, int32_t clear, float* phi_out,
+                                        int32_t* alpha_out) {
+  if (!h) return fail(CUPF_ERR_INVALID, "null handle");
+  if (!h->initialised) return fail(CUPF_ERR_STATE, "state not initialised");
+  CK(cudaSetDevice(h->device));
+  const size_t L = (size_t)h->g.length();
+  if (clear) {
+    CK(cudaMemsetAsync(h->phi_m, 0, L * sizeof(float), h->stream));
+    CK(cudaMemsetAsync(h->alpha_m, 0, L * sizeof(int), h->stream));
+  }
+  cupf_status st = fill_halo(h, h->cur);
+  if (st) return st;
+  collect_kernel<<<grid_for(L), 256, 0, h->stream>>>(h->buf[h->cur], h->phi_m, h->alpha_m, h->g);
+  CK(cudaGetLastError());
+  if (phi_out)
+    CK(cudaMemcpyAsync(phi_out, h->phi_m, L * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  if (alpha_out)
+    CK(cudaMemcpyAsync(alpha_out, h->alpha_m, L * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return check_err_word(h);
+}
+
+extern "C" cupf_status cupf_apt_grain_volumes(cupf_apt_handle* h, int32_t num_grains,
+                                              int64_t* counts) {
+  if (!h || !counts || num_grains < 0) return fail(CUPF_ERR_INVALID, "bad argument");
+  CK(cudaSetDevice(h->device));
+  if (h->counts_cap < num_grains + 1) {
+    if (h->counts) cudaFree(h->counts);
+    if (h->first) cudaFree(h->first);
+    h->counts = nullptr;
+    h->first = nullptr;
+    CK(cudaMalloc((void**)&h->counts, (num_grains + 1) * sizeof(unsigned long long)));
+    CK(cudaMalloc((void**)&h->first, (num_grains + 1) * sizeof(long long)));
+    h->counts_cap = num_grains + 1;
+  }
+  CK(cudaMemsetAsync(h->counts, 0, (num_grains + 1) * sizeof(unsigned long long), h->stream));
+  CK(cudaMemsetAsync(h->first, 0x7F, (num_grains + 1) * sizeof(long long), h->stream));
+  const long long n = (long long)(h->p.fnx - 2) * (h->p.fny - 2) * (h->p.fnz - 2);
+  volume_kernel<<<grid_for(n), 256, 0, h->stream>>>(h->alpha_m, h->p.fnx, h->p.fny, h->p.fnz,
+                                                     num_grains, h->counts, h->first);
+  CK(cudaGetLastError());
+  std::vector<unsigned long long> c(num_grains + 1);
+  CK(cudaMemcpyAsync(c.data(), h->counts, c.size() * sizeof(unsigned long long),
+                     cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int i = 0; i <= num_grains; ++i) counts[i] = (int64_t)c[i];
+  return CUPF_OK;
+}
+
+extern "C" cupf_status cupf_apt_move_domain(cupf_apt_handle* h, int32_t* tip_front,
+                                            int32_t tip_thres, int32_t* move_count,
+                                            int32_t* moved) {
+  if (!h || !tip_front || !move_count || !moved) return fail(CUPF_ERR_INVALID, "null argument");
+  if (!h->initialised) return fail(CUPF_ERR_STATE, "state not initialised");
+  CK(cudaSetDevice(h->device));
+  const Grid& g = h->g;
+  const cupf_apt_params& p = h->p;
+  if (!h->alpha_full) {
+    h->fnz_f = p.fnz * 4 + 8;  // archive capacity in layers; grown on demand below
+    CK(cudaMalloc((void**)&h->alpha_full, (size_t)p.fnx * p.fny * h->fnz_f * sizeof(int)));
+    CK(cudaMemsetAsync(h->alpha_full, 0, (size_t)p.fnx * p.fny * h->fnz_f * sizeof(int),
+                       h->stream));
+    CK(cudaMalloc((void**)&h->loss_area, p.num_theta * sizeof(int)));
+    CK(cudaMemsetAsync(h->loss_area, 0, p.num_theta * sizeof(int), h->stream));
+  }
+  cupf_status st = fill_halo(h, h->cur);
+  if (st) return st;
+  layer_sum_kernel<<<p.fnz, 256, 0, h->stream>>>(h->buf[h->cur], h->layer_sums, g);
+  CK(cudaGetLastError());
+  std::vector<double> sums(p.fnz);
+  CK(cudaMemcpyAsync(sums.data(), h->layer_sums, p.fnz * sizeof(double), cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  // tip_mvf (PhaseField.cu:382-399): first layer whose mean is not above LS
+  const float denom = (float)(p.num_pf * p.fnx * p.fny);
+  while (((double)((float)sums[*tip_front] / denom) > LS) && (*tip_front < p.fnz - 1))
+    (*tip_front)++;
+  *moved = 0;
+  const long long plane = (long long)p.fnx * p.fny;
+  while (*tip_front >= tip_thres) {
+    if (*move_count + 2 > h->fnz_f) {  // grow the archive
+      const int nf = h->fnz_f * 2;
+      int* na = nullptr;
+      CK(cudaMalloc((void**)&na, (size_t)plane * nf * sizeof(int)));
+      CK(cudaMemsetAsync(na, 0, (size_t)plane * nf * sizeof(int), h->stream));
+      CK(cudaMemcpyAsync(na, h->alpha_full, (size_t)plane * h->fnz_f * sizeof(int),
+                         cudaMemcpyDeviceToDevice, h->stream));
+      CK(cudaStreamSynchronize(h->stream));
+      cudaFree(h->alpha_full);
+      h->alpha_full = na;
+      h->fnz_f = nf;
+    }
+    const size_t L = (size_t)g.length();
+    collect_kernel<<<grid_for(L), 256, 0, h->stream>>>(h->buf[h->cur], h->phi_m, h->alpha_m, g);
+    archive_kernel<<<grid_for(plane), 256, 0, h->stream>>>(h->alpha_m, h->alpha_full, h->loss_area,
+                                                           p.fnx, p.fny, *move_count, p.num_theta);
+    const long long ni = (long long)(p.fnx - 2) * (p.fny - 2) * (p.fnz - 2) * p.num_pf;
+    shift_kernel<<<grid_for(ni), 256, 0, h->stream>>>(h->buf[h->cur], h->buf[h->cur ^ 1], g);
+    copy_interior_kernel<<<grid_for(ni), 256, 0, h->stream>>>(h->buf[h->cur ^ 1], h->buf[h->cur],
+                                                              g);
+    CK(cudaGetLastError());
+    // z shift (APTmove_frame :365-369 then APTcopy_frame :401-402)
+    std::vector<float>& z = h->z_host;
+    const float ztop = 2.0f * z[p.fnz - 2] - z[p.fnz - 3];
+    for (int k = 1; k < p.fnz - 2; ++k) z[k] = z[k + 1];
+    z[p.fnz - 2] = ztop;
+    CK(cudaMemcpyAsync(h->z, z.data(), p.fnz * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *move_count += 1;
+    *tip_front -= 1;
+    *moved += 1;
+  }
+  if ((st = fill_halo(h, h->cur))) return st;
+  CK(cudaStreamSynchronize(h->stream));
+  return check_err_word(h);
+}
+
+extern "C" cupf_status cupf_apt_get_archive(cupf_apt_handle* h, int32_t fnz_f, int32_t* alpha_full,
+                                            int32_t* loss_area) {
+  if (!h) return fail(CUPF_ERR_INVALID, "null handle");
+  CK(cudaSetDevice(h->device));
+  const long long plane = (long long)h->p.fnx * h->p.fny;
+  if (alpha_full) {
+    std::memset(alpha_full, 0, (size_t)plane * fnz_f * sizeof(int));
+    if (h->alpha_full) {
+      const int nl = fnz_f < h->fnz_f ? fnz_f : h->fnz_f;
+      CK(cudaMemcpyAsync(alpha_full, h->alpha_full, (size_t)plane * nl * sizeof(int),
+                         cudaMemcpyDeviceToHost, h->stream));
+    }
+  }
+  if (loss_area) {
+    std::memset(loss_area, 0, h->p.num_theta * sizeof(int));
+    if (h->loss_area)
+      CK(cudaMemcpyAsync(loss_area, h->loss_area, h->p.num_theta * sizeof(int),
+                         cudaMemcpyDeviceToHost, h->stream));
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return CUPF_OK;
+}
+
+extern "C" cupf_status cupf_apt_get_z(cupf_apt_handle* h, float* z) {
+  if (!h || !z) return fail(CUPF_ERR_INVALID, "null argument");
+  std::memcpy(z, h->z_host.data(), h->p.fnz * sizeof(float));
+  return CUPF_OK;
+}
+
+extern "C" cupf_status cupf_apt_sync(cupf_apt_handle* h, int32_t timeout_ms) {
+  if (!h) return fail(CUPF_ERR_INVALID, "null handle");
+  CK(cudaSetDevice(h->device));
+  if (timeout_ms <= 0) {
+    CK(cudaStreamSynchronize(h->stream));
+  } else {
+    auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+      cudaError_t e = cudaStreamQuery(h->stream);
+      if (e == cudaSuccess) break;
+      if (e != cudaErrorNotReady) CK(e);
+      auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(
+                    std::chrono::steady_clock::now() - t0)
+                    .count();
+      if (ms > timeout_ms) return fail(CUPF_ERR_TIMEOUT, "stream not idle after %d ms", timeout_ms);
+      std::this_thread::sleep_for(std::chrono::microseconds(200));
+    }
+  }
+  return check_err_word(h);
+}
+
+extern "C" cupf_status cupf_apt_time_steps(cupf_apt_handle* h, int32_t nsteps, float* ms) {
+  if (!h || !ms) return fail(CUPF_ERR_INVALID, "null argument");
+  CK(cudaSetDevice(h->device));
+  CK(cudaEventRecord(h->ev0, h->stream));
+  cupf_status st = cupf_apt_step(h, nsteps, 0);
+  if (st) return st;
+  CK(cudaEventRecord(h->ev1, h->stream));
+  CK(cudaEventSynchronize(h->ev1));
+  CK(cudaEventElapsedTime(ms, h->ev0, h->ev1));
+  return check_err_word(h);
+}

@@ -1,0 +1,214 @@
+/*
+ * cupf.h — C ABI of the B200 APT (active parameter tracking) multi-grain
+ * phase-field step.
+ *
+ * The reference (cuPF, 3DgrainMPI) drives its device step from the C++ class
+ * APTPhaseField.  Every entry point below replaces one device-side method or
+ * kernel-launch group of that class; the citation on each names the reference
+ * code it stands in for (paths are relative to the cuPF repository).
+ *
+ * Conventions
+ *   - Plain C: no C++ or torch types cross this boundary.  Every call returns a
+ *     cupf_status; cupf_last_error() returns a message for the calling thread.
+ *   - Host pointers unless a name ends in "_dev".
+ *   - "Reference layout" means the reference's SoA slot layout:
+ *       index = i + j*fnx + k*fnx*fny + slot*fnx*fny*fnz     (devicefunc.cu_inl:24-29)
+ *     with fnx = nx+1+2 (one halo cell per side), NUM_PF slots per cell,
+ *     phi as float32 and grain ids as int32 (-1 = empty slot).
+ *   - A handle owns its device memory and one CUDA stream.  Calls on different
+ *     handles may run from different host threads; calls on one handle must
+ *     not overlap.
+ */
+#ifndef CUPF_H_
+#define CUPF_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CUPF_ABI_VERSION 1
+#define CUPF_MAX_PF 16
+
+typedef enum cupf_status {
+  CUPF_OK = 0,
+  CUPF_ERR_INVALID = 1,     /* bad argument or unsupported size */
+  CUPF_ERR_CUDA = 2,        /* a CUDA runtime/driver call failed */
+  CUPF_ERR_OOM = 3,         /* device allocation failed */
+  CUPF_ERR_UNSUPPORTED = 4, /* option not built into this library */
+  CUPF_ERR_TIMEOUT = 5,     /* host-side watchdog deadline passed */
+  CUPF_ERR_IO = 6,          /* file could not be read or written */
+  CUPF_ERR_STATE = 7        /* call out of order (e.g. step before init) */
+} cupf_status;
+
+/* Storage precision of the phi slots.  FP32 is the reference's own storage;
+ * BF16 / FP16 store phi in 16 bits and grain ids in int16 while all stencil
+ * arithmetic stays FP32 (the split-precision variant). */
+typedef enum cupf_precision {
+  CUPF_PREC_FP32 = 0,
+  CUPF_PREC_BF16 = 1,
+  CUPF_PREC_FP16 = 2
+} cupf_precision;
+
+/* Parameter block read by the APT step.  Field names and meanings follow the
+ * reference's GlobalConstants (params.h:10-56) as filled by
+ * PhaseField::parseInputParams / cpuSetup (PhaseFieldCpu.cpp:17-374). */
+typedef struct cupf_apt_params {
+  int32_t fnx, fny, fnz;  /* points per axis, halo included */
+  int32_t num_pf;         /* NUM_PF, active slots per cell (1..CUPF_MAX_PF) */
+  int32_t num_theta;      /* NG: grain orientations in sint/cost */
+  int32_t bcX, bcY, bcZ;  /* 0 = no-flux (mirror about 1 / fn-2), 1 = periodic */
+  int32_t thermalType;    /* 0 none, 1 line, 2 cylinder, 3 cone, 4 paraboloid table */
+  int32_t Nx, Ny, Nz, Nt; /* macro thermal grid (thermalType 4, nucleation) */
+  float kin_delta;        /* kinetic anisotropy strength */
+  float eps;              /* |grad phi|^2 threshold in kine_ani */
+  float G;                /* thermal gradient, K/um */
+  float z0;               /* interface height, um */
+  float underCoolingRate; /* UC, K/us */
+  float underCoolingRate0;
+  float L_cp;
+  float hi;               /* 1/dx */
+  float lamd;             /* coupling constant lambda */
+  float dt;               /* dimensionless time step */
+  float tau0;             /* time scale, s */
+  float lyd, lzd;         /* domain lengths, um */
+  float r0, x0, angle, V, mp_len, order;
+  float dx, W0;
+  /* nucleation (used only by the nucleation entry points) */
+  float undcool_mean, undcool_std, nuc_Nmax, nuc_Nmax0, nuc_rad, sqrt2;
+  int32_t pts_cell;
+  int32_t seed;
+  int32_t haloWidth;      /* must be 1 */
+  int32_t reserved[5];
+} cupf_apt_params;
+
+/* Thermal and orientation inputs (the reference's ThermalInputData,
+ * ThermalInputData.h:8-24, plus the coordinate arrays of PDE, cuPDE.h:18-23).
+ * Host arrays; copied to the device by cupf_apt_create. */
+typedef struct cupf_apt_inputs {
+  const float* x;       /* [fnx] */
+  const float* y;       /* [fny] */
+  const float* z;       /* [fnz] */
+  const float* sint;    /* [2*num_theta+1] sinf(theta) */
+  const float* cost;    /* [2*num_theta+1] cosf(theta) */
+  const float* X_mac;   /* [Nx]   (thermalType 4 / nucleation; else NULL) */
+  const float* Y_mac;   /* [Ny] */
+  const float* Z_mac;   /* [Nz] */
+  const float* t_mac;   /* [Nt] */
+  const float* psi_mac; /* [Nx*Ny*Nz] */
+  const float* T_3D;    /* [Nx*Ny*Nz*Nt] (nucleation only; may be NULL) */
+} cupf_apt_inputs;
+
+typedef struct cupf_apt_handle cupf_apt_handle;
+
+/* Message describing the last failure on the calling thread ("" if none). */
+const char* cupf_last_error(void);
+int cupf_abi_version(void);
+/* sizeof of the ABI structs as compiled into the library: which = 0 for
+ * cupf_apt_params, 1 for cupf_apt_inputs (lets bindings check their mirror). */
+size_t cupf_struct_size(int which);
+
+/* Allocate device state and upload parameters and thermal inputs.
+ * Replaces APTPhaseField::cudaSetup (3DgrainMPI/APTPhaseField.cu:569-637).
+ * device: CUDA ordinal.  precision: storage type of the phi slots. */
+cupf_status cupf_apt_create(const cupf_apt_params* p, const cupf_apt_inputs* in,
+                            int device, cupf_precision precision,
+                            cupf_apt_handle** out);
+
+/* Free all device memory of the handle.  Replaces ~APTPhaseField
+ * (3DgrainMPI/APTPhaseField.cu:540-566). */
+cupf_status cupf_apt_destroy(cupf_apt_handle* h);
+
+/* Initialise both slot buffers from the argmax fields phi[length], alpha[length]
+ * (reference layout, length = fnx*fny*fnz): every slot = (-1, -1), then slot 0 =
+ * (phi, alpha) where phi > LS (-0.995).  Resets the step counter and time.
+ * Replaces set_minus1 x2 + APTini_PF x2 + setBC x2 in APTPhaseField::evolve
+ * (3DgrainMPI/APTPhaseField.cu:727-728, 771-772, 817-818; PhaseField.cu:51-57). */
+cupf_status cupf_apt_init_from_argmax(cupf_apt_handle* h, const float* phi,
+                                      const int32_t* alpha);
+
+/* Load a full slot state (reference layout, num_pf*length entries) into the
+ * "old" buffer, i.e. the buffer the next step reads.  kt_half is the number of
+ * explicit steps already taken (sets the time of the next step). */
+cupf_status cupf_apt_set_slots(cupf_apt_handle* h, const float* ph,
+                               const int32_t* ids, int64_t steps_done);
+
+/* Export the current slot state in reference layout with the halo filled by the
+ * boundary rule (what APTsetBC3D leaves in PFs_old / active_args_old).
+ * Replaces the D2H copies of APTPhaseField::getLineQoIs
+ * (3DgrainMPI/APTPhaseField.cu:666-667) preceded by setBC (:700-707). */
+cupf_status cupf_apt_get_slots(cupf_apt_handle* h, float* ph, int32_t* ids);
+
+/* Advance nsteps explicit Euler steps.  Each step reads the current buffer,
+ * applies the boundary rule to its halo, and writes the other buffer; the time
+ * of step n (1-based, counted from the last init) is t = n*dt*tau0 in float,
+ * as the reference forms (2*kt+1)*dt*tau0 and (2*kt+2)*dt*tau0.
+ * Replaces the APTsetBC3D + APTrhs_psi launches of APTPhaseField::evolve
+ * (3DgrainMPI/APTPhaseField.cu:861-864, 880, 919-920; kernels :93-174, :178-354).
+ * use_initial_undercooling selects the reference's liquid-start temperature
+ * (Tinterp = -underCoolingRate0*1e6*t, :280-283). */
+cupf_status cupf_apt_step(cupf_apt_handle* h, int32_t nsteps,
+                          int32_t use_initial_undercooling);
+
+/* Number of explicit steps taken since the last init / set_slots. */
+cupf_status cupf_apt_steps_done(cupf_apt_handle* h, int64_t* steps);
+
+/* Per-cell argmax over the slots of the current buffer: where the max phi is
+ * above LS, phi_out[C] = max and alpha_out[C] = its grain id (first slot wins
+ * ties); elsewhere the cell keeps the value it had in the device argmax buffer,
+ * which cupf_apt_collect clears to (phi 0, alpha 0) first when clear != 0.
+ * Either output may be NULL.  Replaces APTcollect_PF + cudaMemcpy
+ * (3DgrainMPI/APTPhaseField.cu:55-75, 820-822, 907-909). */
+cupf_status cupf_apt_collect(cupf_apt_handle* h, int32_t clear, float* phi_out,
+                             int32_t* alpha_out);
+
+/* Voxel count of every grain id 1..num_grains over the interior cells of the
+ * argmax map computed by the last cupf_apt_collect (alpha > 0 only), FP64-free
+ * integer reduction on the device.  counts has num_grains+1 entries; counts[0]
+ * receives the number of interior cells with alpha <= 0 or alpha > num_grains.
+ * The per-grain volumes of QOI::calculateQoIs (3DgrainMPI/QOI.cpp:198-231). */
+cupf_status cupf_apt_grain_volumes(cupf_apt_handle* h, int32_t num_grains,
+                                   int64_t* counts);
+
+/* Moving-domain check and shift (line configuration).  Computes the per-layer
+ * mean of phi over all slots and cells, advances *tip_front while the mean is
+ * above LS, and while *tip_front >= tip_thres shifts the window down one layer:
+ * archives the bottom interior alpha layer into alpha_full[move_count] (device
+ * archive of fnz_f layers), adds its cells to loss_area, sets the new top
+ * interior layer to (-1, -1) and shifts z.  Ends with the boundary fill and a
+ * fresh argmax.  *moved receives the number of layers shifted.
+ * Replaces APTPhaseField::moveDomain + tip_mvf + APTmove_frame + APTcopy_frame
+ * (3DgrainMPI/APTPhaseField.cu:678-697, 357-410; PhaseField.cu:366-399). */
+cupf_status cupf_apt_move_domain(cupf_apt_handle* h, int32_t* tip_front,
+                                 int32_t tip_thres, int32_t* move_count,
+                                 int32_t* moved);
+
+/* Read back the archive of evicted alpha layers (fnx*fny*fnz_f ints) and the
+ * per-grain lost area (num_theta ints); either pointer may be NULL.
+ * The D2H copies of APTPhaseField::getLineQoIs / evolve
+ * (3DgrainMPI/APTPhaseField.cu:668, 912). */
+cupf_status cupf_apt_get_archive(cupf_apt_handle* h, int32_t fnz_f,
+                                 int32_t* alpha_full, int32_t* loss_area);
+
+/* Current z coordinates (fnz floats), shifted by cupf_apt_move_domain. */
+cupf_status cupf_apt_get_z(cupf_apt_handle* h, float* z);
+
+/* Wait for all work queued on the handle's stream, failing with
+ * CUPF_ERR_TIMEOUT after timeout_ms milliseconds (<= 0: wait forever). */
+cupf_status cupf_apt_sync(cupf_apt_handle* h, int32_t timeout_ms);
+
+/* Time nsteps steps with CUDA events on the handle's stream (warm state, no
+ * host copies).  *ms receives the elapsed device time. */
+cupf_status cupf_apt_time_steps(cupf_apt_handle* h, int32_t nsteps, float* ms);
+
+/* Raw stream of the handle (a cudaStream_t), for callers that order their own
+ * work after the solver's. */
+void* cupf_apt_stream(cupf_apt_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUPF_H_ */

@@ -1,0 +1,138 @@
+"""Build recipe for the test oracle (TEST INFRASTRUCTURE ONLY).
+
+Outputs
+  oracle/liboracle.so           C restatement of the APT step (apt_oracle.c)
+  oracle/_ref/libref_host.so    reference host code (QOI.cpp, helper.cpp,
+                                DesignSettingData.cpp) compiled unmodified, with
+                                an extern "C" shim (ref/ref_host_shim.cpp)
+  oracle/_ref/libref_apt5.so    reference kernels (APTPhaseField.cu, PhaseField.cu,
+                                ...) compiled for sm_100a, NUM_PF=5 as shipped,
+                                with launchers (ref/ref_harness.cu)
+  oracle/_ref/libref_aptN.so    the same with APT_NUM_PF set to N (N = 1..8)
+
+APTPhaseField.cu is compiled from a generated copy (oracle/_ref/srcN/, never
+committed) with exactly two textual edits:
+  1. APT_NUM_PF set to N (the reference hard-codes the slot count, :30);
+  2. local_phs declared with 8 rows instead of 7 (:199).  When more than NUM_PF
+     distinct grain ids meet, the reference's merge writes local_phs[6][NUM_PF],
+     one element past the array (:222-231).  What that overwrites depends on the
+     compiler's stack layout and may be the id list itself, after which the id
+     indexes the orientation table out of bounds.  With the padding row the
+     stray write lands in unused storage: the entry is dropped, which is the
+     behaviour the oracle and the library define for this case.
+Every other file is compiled unmodified from where it lies (REF_DIR); nothing is
+copied into the repository.  The _ref outputs are built only when the reference
+tree exists; on a machine without it the prebuilt files are used as they are.
+"""
+import os
+import shutil
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+REF_DIR = os.environ.get("CUPF_REFERENCE_DIR", "/root/reference/3DgrainMPI")
+OUT = os.path.join(HERE, "_ref")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+CUDA_INC = "/usr/local/cuda/include"
+CUDA_LIB = "/usr/local/cuda/lib64"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("build failed: %s\n%s%s" % (" ".join(cmd), r.stdout, r.stderr))
+
+
+def _newer(target, sources):
+    if not os.path.exists(target):
+        return False
+    t = os.path.getmtime(target)
+    return all(os.path.getmtime(s) <= t for s in sources if os.path.exists(s))
+
+
+def build_oracle(force=False):
+    src = os.path.join(HERE, "apt_oracle.c")
+    out = os.path.join(HERE, "liboracle.so")
+    hdr = os.path.join(ROOT, "include", "cupf.h")
+    if force or not _newer(out, [src, hdr, __file__]):
+        _run(["gcc", "-O2", "-std=c11", "-fopenmp", "-ffp-contract=off", "-fPIC", "-shared",
+              src, "-o", out, "-lm"])
+    return out
+
+
+def build_ref_host(force=False):
+    if not os.path.isdir(REF_DIR):
+        return None
+    os.makedirs(OUT, exist_ok=True)
+    out = os.path.join(OUT, "libref_host.so")
+    srcs = [os.path.join(REF_DIR, f) for f in ("QOI.cpp", "helper.cpp", "DesignSettingData.cpp")]
+    shim = os.path.join(HERE, "ref", "ref_host_shim.cpp")
+    if force or not _newer(out, srcs + [shim, __file__]):
+        _run(["g++", "-O2", "-std=c++14", "-fPIC", "-shared", "-w", "-I", REF_DIR,
+              "-I", os.path.join(HERE, "ref"), "-I", CUDA_INC] + srcs + [shim, "-o", out,
+              "-L", CUDA_LIB, "-lcudart", "-Wl,-rpath," + CUDA_LIB])
+    return out
+
+
+def build_ref_gpu(num_pf, force=False):
+    if not os.path.isdir(REF_DIR):
+        return None
+    os.makedirs(OUT, exist_ok=True)
+    out = os.path.join(OUT, "libref_apt%d.so" % num_pf)
+    harness = os.path.join(HERE, "ref", "ref_harness.cu")
+    apt = os.path.join(REF_DIR, "APTPhaseField.cu")
+    d = os.path.join(OUT, "src%d" % num_pf)
+    os.makedirs(d, exist_ok=True)
+    text = open(apt).read()
+    edits = [("#define APT_NUM_PF 5", "#define APT_NUM_PF %d" % num_pf),
+             ("float local_phs[7][APT_NUM_PF];", "float local_phs[8][APT_NUM_PF];")]
+    for old, new in edits:
+        assert text.count(old) == 1, "reference text not found: " + old
+        text = text.replace(old, new)
+    gen = os.path.join(d, "APTPhaseField.cu")
+    if not os.path.exists(gen) or open(gen).read() != text:
+        with open(gen, "w") as f:
+            f.write(text)
+    inc = ["-I", d]
+    cu = [harness] + [os.path.join(REF_DIR, f) for f in ("PhaseField.cu", "MPIsettingCuda.cu")]
+    cpp = [os.path.join(REF_DIR, f) for f in ("helper.cpp", "QOI.cpp", "MovingDomain.cpp",
+                                                 "MPIsetting.cpp", "DesignSettingData.cpp",
+                                                 "ThermalInputData.cpp")]
+    cpp.append(os.path.join(HERE, "ref", "ref_host_stubs.cpp"))
+    deps = cu + cpp + [apt, __file__, os.path.join(HERE, "ref", "mpi.h")]
+    if not force and _newer(out, deps):
+        return out
+    objdir = os.path.join(OUT, "obj%d" % num_pf)
+    os.makedirs(objdir, exist_ok=True)
+    common = ["-I", os.path.join(HERE, "ref")] + inc + ["-I", REF_DIR]
+    jobs = []
+    for s in cu:
+        o = os.path.join(objdir, os.path.basename(s) + ".o")
+        jobs.append([NVCC] + ARCH + ["-O3", "-std=c++14", "-w", "-Xcompiler", "-fPIC",
+                                     "-lineinfo", "-c", s, "-o", o] + common)
+    for s in cpp:
+        o = os.path.join(objdir, os.path.basename(s) + ".o")
+        jobs.append(["g++", "-O3", "-std=c++14", "-w", "-fPIC", "-c", s, "-o", o, "-I",
+                     CUDA_INC] + common)
+    with ThreadPoolExecutor(max_workers=8) as ex:
+        list(ex.map(_run, jobs))
+    objs = [j[j.index("-o") + 1] for j in jobs]
+    _run([NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", out] + objs +
+         ["-lcudart", "-Xlinker", "--no-undefined"])
+    return out
+
+
+def build_all(force=False):
+    outs = [build_oracle(force)]
+    outs.append(build_ref_host(force))
+    with ThreadPoolExecutor(max_workers=2) as ex:
+        outs += list(ex.map(lambda n: build_ref_gpu(n, force), range(1, 9)))
+    return outs
+
+
+if __name__ == "__main__":
+    for o in build_all(force="--force" in sys.argv):
+        print(o)

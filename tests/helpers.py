@@ -1,0 +1,77 @@
+"""Shared test helpers: run the reference kernels and compare states."""
+import numpy as np
+
+from cupf_b200 import cases
+
+EDGE_CACHE = {}
+
+
+def face_mask(p):
+    """Boolean mask (reference layout, one slot) of interior cells and face-halo
+    cells; cells on two or three halo faces (edges, corners) are excluded
+    because the reference fills them with racing threads."""
+    key = (p.fnx, p.fny, p.fnz)
+    if key not in EDGE_CACHE:
+        k, j, i = np.meshgrid(np.arange(p.fnz), np.arange(p.fny), np.arange(p.fnx), indexing="ij")
+        nh = ((i == 0) | (i == p.fnx - 1)).astype(int) + ((j == 0) | (j == p.fny - 1)) + \
+             ((k == 0) | (k == p.fnz - 1))
+        EDGE_CACHE[key] = (nh <= 1).reshape(-1)
+    return EDGE_CACHE[key]
+
+
+def interior_mask(p):
+    k, j, i = np.meshgrid(np.arange(p.fnz), np.arange(p.fny), np.arange(p.fnx), indexing="ij")
+    m = (i > 0) & (i < p.fnx - 1) & (j > 0) & (j < p.fny - 1) & (k > 0) & (k < p.fnz - 1)
+    return m.reshape(-1)
+
+
+def compare_states(p, ph_a, id_a, ph_b, id_b, mask=None):
+    """Return (n_id_mismatch, n_phi_bit_mismatch, max_abs_phi_diff) over mask."""
+    m = face_mask(p) if mask is None else mask
+    m = np.tile(m, p.num_pf)
+    ida, idb = id_a[m], id_b[m]
+    pa, pb = ph_a[m], ph_b[m]
+    n_id = int(np.count_nonzero(ida != idb))
+    n_ph = int(np.count_nonzero(pa.view(np.int32) != pb.view(np.int32)))
+    d = float(np.max(np.abs(pa.astype(np.float64) - pb.astype(np.float64)))) if pa.size else 0.0
+    return n_id, n_ph, d
+
+
+def run_reference_gpu(case, nsteps, use_iuc=False, ph0=None, id0=None):
+    """Run the reference kernels (RefGPU) nsteps from the initial slots; return
+    the boundary-filled final state (numpy, reference layout)."""
+    import torch
+    from oracle import RefGPU
+    p = case.params
+    ref = RefGPU(p.num_pf)
+    ref.check(ref.L.ref_set_params(p))
+    if ph0 is None:
+        ph0, id0 = case.initial_slots()
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    x, y, z, sint, cost = (dev(a) for a in (case.x, case.y, case.z, case.sint, case.cost))
+    a_ph, a_id, b_ph, b_id = dev(ph0), dev(id0), dev(ph0), dev(id0)
+    for n in range(1, nsteps + 1):
+        t = np.float32(np.float32(n) * np.float32(p.dt)) * np.float32(p.tau0)
+        ref.check(ref.L.ref_set_bc(a_ph.data_ptr(), a_id.data_ptr()))
+        ref.check(ref.L.ref_rhs_psi(float(t), x.data_ptr(), y.data_ptr(), z.data_ptr(),
+                                    a_ph.data_ptr(), b_ph.data_ptr(), a_id.data_ptr(),
+                                    b_id.data_ptr(), sint.data_ptr(), cost.data_ptr(), None, None,
+                                    None, None, None, None, int(use_iuc)))
+        a_ph, b_ph = b_ph, a_ph
+        a_id, b_id = b_id, a_id
+    ref.check(ref.L.ref_set_bc(a_ph.data_ptr(), a_id.data_ptr()))
+    torch.cuda.synchronize()
+    out = a_ph.cpu().numpy(), a_id.cpu().numpy()
+    del a_ph, a_id, b_ph, b_id
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_cupf(case, nsteps, use_iuc=False, ph0=None, id0=None):
+    from cupf_b200.solver import APTSolver
+    if ph0 is None:
+        ph0, id0 = case.initial_slots()
+    with APTSolver(case) as s:
+        s.set_slots(ph0, id0, 0)
+        s.step(nsteps, use_iuc)
+        return s.get_slots()
