@@ -41,13 +41,13 @@ LINE_CONSTANTS = dict(Tmelt=933.3, Dh=8.43e7, L_cp=229.0, GT=0.347, beta0=1e-7, 
 def derive_params(c: dict) -> dict:
     """Derived parameters with the reference's rounding (PhaseFieldCpu.cpp:141-172)."""
     f = {k: F32(v) for k, v in c.items() if isinstance(v, float)}
-    R = float(c["R"])  # m/s, compared in float
+    R = np.float64(F32(c["R"]))  # m/s: a float compared with double literals
     cfl = f["cfl"]
     uc0 = f["underCoolingRate0"]
-    if F32(R) < F32(0.3):
+    if R < 0.3:
         cfl = F32(cfl * F32(2))
         uc0 = F32(uc0 / F32(2))
-    if F32(R) > F32(0.3) and F32(R) < F32(1.0):
+    if R > 0.3 and R < 1.0:
         cfl = F32(np.float64(cfl) * 1.5)
         uc0 = F32(np.float64(uc0) / 1.5)
     d0 = F32(f["GT"] / f["L_cp"])

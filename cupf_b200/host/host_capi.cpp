@@ -1,0 +1,143 @@
+// host_capi.cpp — C entry points of include/cupf_host.h.
+#include <cstring>
+#include <string>
+
+#include "../../include/cupf_host.h"
+#include "host_util.h"
+#include "phase_field.h"
+#include "qoi.h"
+
+using namespace cupf_host;
+
+extern "C" int cupf_host_grain_volumes(int fnx, int fny, int fnz, const int32_t* alpha,
+                                       int32_t* grain_ids, int32_t* volumes, int cap) {
+  QoiGrid g;
+  g.fnx = fnx;
+  g.fny = fny;
+  g.fnz = fnz;
+  QOI3D q(g);
+  q.calculateQoIs(g, alpha, 0);
+  const int n = q.mNumActiveGrains;
+  if (n > cap) return -1;
+  for (int i = 0; i < n; ++i) {
+    grain_ids[i] = q.mQoIVectorIntData["grainToPF"][i];
+    volumes[i] = q.mQoIVectorIntData["volume"][i];
+  }
+  return n;
+}
+
+extern "C" int cupf_host_line_qois(int fnx, int fny, int fnz, int num_theta, int* cur_tip,
+                                   const int32_t* alpha, const int32_t* loss_area, int move_count,
+                                   int32_t* tip_y, int32_t* total_area, int32_t* extra_area) {
+  QoiGrid g;
+  g.fnx = fnx;
+  g.fny = fny;
+  g.fnz = fnz;
+  g.num_theta = num_theta;
+  g.nts = 0;
+  QOILine q(g);
+  q.calculateLineQoIs(g, *cur_tip, alpha, 0, nullptr, loss_area, move_count);
+  *tip_y = q.mQoIVectorIntData["tip_y"][0];
+  for (int i = 0; i < num_theta; ++i) {
+    total_area[i] = q.mQoIVectorIntData["total_area"][i];
+    extra_area[i] = q.mQoIVectorIntData["extra_area"][i];
+  }
+  return 0;
+}
+
+extern "C" int cupf_host_sample_heights(int* cur_tip, const int32_t* alpha, int fnx, int fny,
+                                        int fnz) {
+  QoiGrid g;
+  QOI3D q(g);
+  q.sampleHeights(*cur_tip, alpha, fnx, fny, fnz);
+  return 0;
+}
+
+extern "C" int cupf_host_junctions_3d(int fnx, int fny, int fnz, const int32_t* alpha,
+                                      int32_t* nodes, int cap) {
+  QoiGrid g;
+  g.fnx = fnx;
+  g.fny = fny;
+  g.fnz = fnz;
+  QOI3D q(g);
+  q.calculateQoIs(g, alpha, 0);
+  q.searchJunctionsOnImage(g, alpha);
+  const std::vector<int>& v = q.mQoIVectorIntData["node_region"];
+  const int n = (int)v.size();
+  for (int i = 0; i < n && i < cap; ++i) nodes[i] = v[i];
+  return n;
+}
+
+extern "C" int cupf_host_get_param_float(const char* line, const char* key, float* value) {
+  return getParam(std::string(line), std::string(key), *value) ? 1 : 0;
+}
+
+extern "C" int cupf_host_get_param_int(const char* line, const char* key, int32_t* value) {
+  int v = *value;
+  const bool ok = getParam(std::string(line), std::string(key), v);
+  *value = v;
+  return ok ? 1 : 0;
+}
+
+extern "C" int cupf_host_get_options(int argc, char** argv, int32_t* out, char* input_file,
+                                     char* folder, char* outdir, int cap) {
+  DesignSettingData d;
+  if (!d.getOptions(argc, argv)) return -1;
+  out[0] = d.useLineConfig;
+  out[1] = d.includeNucleation;
+  out[2] = d.pureNucleation;
+  out[3] = d.useAPT;
+  out[4] = d.save3DField;
+  out[5] = d.mpiDim;
+  out[6] = d.seedValue;
+  out[7] = d.bcX;
+  out[8] = d.bcY;
+  out[9] = d.bcZ;
+  std::strncpy(input_file, d.inputFile.c_str(), cap);
+  std::strncpy(folder, d.thermalInputFolder.c_str(), cap);
+  std::strncpy(outdir, d.outputFolder.c_str(), cap);
+  return 0;
+}
+
+namespace {
+class SetupOnly : public PhaseField {
+ public:
+  bool cudaSetup() override { return true; }
+  bool evolve() override { return true; }
+};
+}  // namespace
+
+extern "C" int cupf_host_setup(const char* input_file, const char* folder, int bcX, int bcY,
+                               int bcZ, int flags, int32_t* dims, float* fparams, float* phi,
+                               int32_t* alpha, int64_t length_cap, char* err, int err_cap) {
+  DesignSettingData ds;
+  ds.inputFile = input_file;
+  ds.useLineConfig = (flags & 1) != 0;
+  ds.pureNucleation = (flags & 2) != 0;
+  ds.bcX = bcX;
+  ds.bcY = bcY;
+  ds.bcZ = bcZ;
+  SetupOnly pf;
+  pf.SetDesignSetting(&ds);
+  pf.mac.folder = folder;
+  std::string path = input_file;
+  // the thermal type is chosen by the input file's name; the file itself may
+  // live elsewhere: try the folder's parent when the bare name does not open
+  bool ok = pf.parseInputParams(path) && pf.cpuSetup() && pf.initField();
+  if (!ok) {
+    if (err && err_cap > 0) std::strncpy(err, pf.lastError().c_str(), err_cap);
+    return -1;
+  }
+  dims[0] = pf.fnx;
+  dims[1] = pf.fny;
+  dims[2] = pf.fnz;
+  dims[3] = pf.params.num_theta;
+  const GlobalConstants& p = pf.params;
+  const float fp[8] = {p.dt, p.tau0, p.lamd, p.hi, p.G, p.underCoolingRate, p.z0, p.kin_delta};
+  std::memcpy(fparams, fp, sizeof(fp));
+  if (phi && alpha && length_cap >= pf.length) {
+    std::memcpy(phi, pf.phi.data(), sizeof(float) * pf.length);
+    std::memcpy(alpha, pf.alpha.data(), sizeof(int) * pf.length);
+  }
+  return 0;
+}

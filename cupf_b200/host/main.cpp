@@ -1,0 +1,39 @@
+// phase_field — command-line driver with the reference's call order
+// (3DgrainMPI/main.cpp:15-77): options, solver, parseInputParams, cpuSetup, QoI
+// object, initField, cudaSetup, evolve, OutputQoIs.  Single process, one GPU.
+#include <cstdio>
+#include <memory>
+
+#include "phase_field.h"
+
+using namespace cupf_host;
+
+int main(int argc, char** argv) {
+  DesignSettingData ds;
+  std::string err;
+  if (!ds.getOptions(argc, argv, &err)) {
+    std::fprintf(stderr, "%s\n", err.c_str());
+    return 2;
+  }
+  if (!ds.useAPT) {
+    std::fprintf(stderr, "the full (non-APT) phase-field mode is not built\n");
+    return 2;
+  }
+  std::unique_ptr<APTPhaseField> pf(new APTPhaseField());
+  pf->SetDesignSetting(&ds);
+  pf->mac.folder = ds.thermalInputFolder + std::to_string(ds.seedValue);
+  pf->params.seed_val = ds.seedValue;
+  bool ok = pf->parseInputParams(ds.inputFile) && pf->cpuSetup();
+  if (ok) {
+    if (ds.useLineConfig) pf->qois.reset(new QOILine(pf->qoiGrid()));
+    else pf->qois.reset(new QOI3D(pf->qoiGrid()));
+    ok = pf->initField() && pf->cudaSetup() && pf->evolve() && pf->OutputQoIs();
+  }
+  if (!ok) {
+    std::fprintf(stderr, "phase_field: %s\n", pf->lastError().c_str());
+    return 1;
+  }
+  std::printf("phase_field: %d steps, walltime %d s, %d grains active\n", pf->params.Mt,
+              pf->params.walltime, pf->qois->mNumActiveGrains);
+  return 0;
+}

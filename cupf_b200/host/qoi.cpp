@@ -1,0 +1,196 @@
+// qoi.cpp — host quantities of interest (see qoi.h).
+//
+// Algorithms restated from the reference QOI.cpp; the containers whose
+// iteration order reaches the output (the std::unordered_map of the junction
+// search) are the same standard containers used the same way, so the order of
+// the grain ids written per junction is identical for the same C++ library.
+// Differences, each a bound the reference lacks: the tip scans stop at the top
+// interior layer, ids outside 1..NG are not counted into per-grain arrays, and
+// junction lists stop at their preallocated capacity.
+#include "qoi.h"
+
+#include <algorithm>
+#include <unordered_map>
+
+namespace cupf_host {
+
+static inline bool layer_has_liquid(const int* alpha, int fnx, int fny, int k) {
+  const long long off = (long long)fnx * fny * k;
+  for (int j = 1; j < fny - 1; ++j)
+    for (int i = 1; i < fnx - 1; ++i)
+      if (alpha[off + (long long)j * fnx + i] == 0) return true;
+  return false;
+}
+
+// QOI::sampleHeights (QOI.cpp:162-185): advance to the last fully solid layer.
+void QOI::sampleHeights(int& cur_tip, const int* alpha, int fnx, int fny, int fnz) {
+  for (;;) {
+    cur_tip += 1;
+    if (cur_tip >= fnz - 1 || layer_has_liquid(alpha, fnx, fny, cur_tip)) break;
+  }
+  cur_tip -= 1;
+}
+
+QOILine::QOILine(const QoiGrid& g) {
+  const int frames = g.nts + 1;
+  mQoIVectorFloatData["fractions"] = std::vector<float>((size_t)frames * g.num_theta);
+  mQoIVectorIntData["tip_y"] = std::vector<int>(frames);
+  mQoIVectorIntData["cross_sec"] = std::vector<int>();
+  mQoIVectorIntData["extra_area"] = std::vector<int>((size_t)frames * g.num_theta, 0);
+  mQoIVectorIntData["total_area"] = std::vector<int>((size_t)frames * g.num_theta, 0);
+  mQoIVectorIntData["tip_final"] = std::vector<int>((size_t)frames * g.num_theta);
+  const int repeated_index = 5;
+  mQoIVectorIntData["node_region"] =
+      std::vector<int>((size_t)frames * repeated_index * g.num_nodes * mNumNodeFeatures, -1);
+}
+
+// QOI::calculateLineQoIs (QOI.cpp:38-101)
+void QOI::calculateLineQoIs(const QoiGrid& g, int& cur_tip, const int* alpha, int kt,
+                            const float* /*z*/, const int* loss_area, int move_count) {
+  const int fnx = g.fnx, fny = g.fny, fnz = g.fnz, ng = g.num_theta;
+  sampleHeights(cur_tip, alpha, fnx, fny, fnz);
+  mQoIVectorIntData["tip_y"][kt] = cur_tip + move_count;
+  std::vector<int>& total = mQoIVectorIntData["total_area"];
+  std::vector<int>& extra = mQoIVectorIntData["extra_area"];
+  for (int k = 1; k < fnz - 1; ++k) {
+    const long long off = (long long)fnx * fny * k;
+    for (int j = 1; j < fny - 1; ++j)
+      for (int i = 1; i < fnx - 1; ++i) {
+        const int a = alpha[off + (long long)fnx * j + i];
+        if (a > 0 && a <= ng) {
+          total[(size_t)kt * ng + a - 1] += 1;
+          if (k > cur_tip) extra[(size_t)kt * ng + a - 1] += 1;
+        }
+      }
+  }
+  for (int j = 0; j < ng; ++j) total[(size_t)kt * ng + j] += loss_area[j];
+}
+
+// QOILine::searchJunctionsOnImage (QOI.cpp:103-160): per saved tip layer, the
+// cross section and the 3x3 in-plane neighbourhoods with >= 3 grains.
+void QOILine::searchJunctionsOnImage(const QoiGrid& g, const int* alpha) {
+  const int fnx = g.fnx, fny = g.fny;
+  std::vector<int>& node = mQoIVectorIntData["node_region"];
+  std::vector<int>& cross = mQoIVectorIntData["cross_sec"];
+  const std::vector<int>& tip_y = mQoIVectorIntData["tip_y"];
+  for (int kt = 0; kt < g.nts + 1; ++kt) {
+    const int cur_tip = tip_y[kt];
+    const long long off = (long long)fnx * fny * cur_tip;
+    cross.insert(cross.end(), alpha + off, alpha + off + (long long)fnx * fny);
+    const size_t base = node.size() / (g.nts + 1) * kt;
+    const size_t cap = node.size() / (g.nts + 1);
+    size_t node_cnt = 0;
+    for (int j = 1; j < fny - 1; ++j)
+      for (int i = 1; i < fnx - 1; ++i) {
+        std::unordered_map<int, int> occur;
+        for (int dj = -1; dj <= 1; ++dj)
+          for (int di = -1; di <= 1; ++di) {
+            const int v = alpha[off + (long long)(j + dj) * fnx + i + di];
+            auto it = occur.find(v);
+            if (it != occur.end())
+              it->second++;
+            else
+              occur.insert({v, 1});
+          }
+        int n_alpha = 0, max_occ = 0;
+        for (auto& it : occur) {
+          n_alpha++;
+          max_occ = std::max(max_occ, it.second);
+        }
+        if (n_alpha >= 3 && max_occ <= 5) {
+          if ((node_cnt + 1) * mNumNodeFeatures > cap) continue;
+          const size_t o = base + node_cnt * mNumNodeFeatures;
+          node[o] = i;
+          node[o + 1] = j;
+          node[o + 2] = max_occ;
+          int c = 0;
+          for (auto& it : occur)
+            if (3 + c < mNumNodeFeatures) node[o + 3 + c++] = it.first;
+          node_cnt++;
+        }
+      }
+  }
+}
+
+QOI3D::QOI3D(const QoiGrid&) {
+  mQoIVectorIntData["volume"] = std::vector<int>();
+  mQoIVectorIntData["grainToPF"] = std::vector<int>();
+  mQoIVectorIntData["node_region"] = std::vector<int>();
+  mQoIVectorIntData["manifold"] = std::vector<int>();
+  mQoIVectorFloatData["geodesic_y_coors"] = std::vector<float>();
+}
+
+// QOI::calculateQoIs (QOI.cpp:198-231): voxel count of every grain id > 0 over
+// the interior, grains listed in order of first occurrence in (k, j, i) order.
+void QOI::calculateQoIs(const QoiGrid& g, const int* alpha, int /*kt*/) {
+  std::vector<int>& vol = mQoIVectorIntData["volume"];
+  std::vector<int>& g2p = mQoIVectorIntData["grainToPF"];
+  vol.clear();
+  g2p.clear();
+  std::unordered_map<int, int> index;
+  mNumActiveGrains = 0;
+  for (int k = 1; k < g.fnz - 1; ++k) {
+    const long long off = (long long)g.fnx * g.fny * k;
+    for (int j = 1; j < g.fny - 1; ++j)
+      for (int i = 1; i < g.fnx - 1; ++i) {
+        const int a = alpha[off + (long long)g.fnx * j + i];
+        if (a <= 0) continue;
+        auto it = index.find(a);
+        if (it == index.end()) {
+          it = index.insert({a, mNumActiveGrains++}).first;
+          g2p.push_back(a);
+          vol.push_back(0);
+        }
+        vol[it->second] += 1;
+      }
+  }
+}
+
+// QOI3D::searchJunctionsOnImage (QOI.cpp:233-311): solid cells whose
+// 19-point neighbourhood (|d|^2 <= 2) holds no liquid and exactly 4 grains.
+void QOI3D::searchJunctionsOnImage(const QoiGrid& g, const int* alpha) {
+  const int fnx = g.fnx, fny = g.fny, fnz = g.fnz;
+  std::vector<int>& node = mQoIVectorIntData["node_region"];
+  node.assign((size_t)40 * mNumActiveGrains * mNumNodeFeatures, -1);
+  size_t node_cnt = 0;
+  std::unordered_map<int, int> occur;
+  for (int k = 1; k < fnz - 1; ++k)
+    for (int j = 1; j < fny - 1; ++j)
+      for (int i = 1; i < fnx - 1; ++i) {
+        const long long C = (long long)k * fnx * fny + (long long)j * fnx + i;
+        if (alpha[C] == 0) continue;
+        occur.clear();
+        int zeros = 0;
+        for (int dk = -1; dk <= 1; ++dk)
+          for (int dj = -1; dj <= 1; ++dj)
+            for (int di = -1; di <= 1; ++di) {
+              if (di * di + dj * dj + dk * dk > 2) continue;
+              const int v = alpha[(long long)(k + dk) * fnx * fny + (long long)(j + dj) * fnx + i + di];
+              if (v == 0) zeros++;
+              auto it = occur.find(v);
+              if (it != occur.end())
+                it->second++;
+              else
+                occur.insert({v, 1});
+            }
+        if (zeros > 0) continue;
+        int n_alpha = 0, max_occ = 0;
+        for (auto& it : occur) {
+          n_alpha++;
+          max_occ = std::max(max_occ, it.second);
+        }
+        if (n_alpha == 4 && max_occ <= 10) {
+          if ((node_cnt + 1) * mNumNodeFeatures > node.size()) continue;
+          const size_t o = node_cnt * mNumNodeFeatures;
+          node[o] = i;
+          node[o + 1] = j;
+          node[o + 2] = k;
+          node[o + 3] = max_occ;
+          int c = 0;
+          for (auto& it : occur) node[o + 4 + c++] = it.first;
+          node_cnt++;
+        }
+      }
+}
+
+}  // namespace cupf_host

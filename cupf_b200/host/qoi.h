@@ -1,0 +1,56 @@
+// qoi.h — quantities of interest of the APT driver, on host argmax maps.
+//
+// Same names, inputs and outputs as the reference's QOI classes
+// (3DgrainMPI/QOI.h:12-48, QOI.cpp): per-grain voxel volumes in first-seen
+// order (calculateQoIs), the line-configuration tip / total / extra areas
+// (calculateLineQoIs), the tip sampler (sampleHeights) and the junction search
+// on the argmax map (searchJunctionsOnImage, line and 3D variants).  Maps are in
+// the reference layout (index i + j*fnx + k*fnx*fny).
+#pragma once
+
+#include <map>
+#include <string>
+#include <vector>
+
+namespace cupf_host {
+
+struct QoiGrid {
+  int fnx = 0, fny = 0, fnz = 0;
+  int num_theta = 0;  // NG
+  int nts = 0;        // number of QoI frames (frames 0..nts)
+  int num_nodes = 0;  // NN (line junction capacity)
+};
+
+class QOI {
+ public:
+  virtual ~QOI() = default;
+  virtual void searchJunctionsOnImage(const QoiGrid& g, const int* alpha) = 0;
+  void calculateLineQoIs(const QoiGrid& g, int& cur_tip, const int* alpha, int kt, const float* z,
+                         const int* loss_area, int move_count);
+  void calculateQoIs(const QoiGrid& g, const int* alpha, int kt);
+  void sampleHeights(int& cur_tip, const int* alpha, int fnx, int fny, int fnz);
+
+  std::map<std::string, std::vector<int>> mQoIVectorIntData;
+  std::map<std::string, std::vector<float>> mQoIVectorFloatData;
+  int mNumActiveGrains = 0;
+};
+
+class QOILine : public QOI {
+ public:
+  explicit QOILine(const QoiGrid& g);
+  void searchJunctionsOnImage(const QoiGrid& g, const int* alpha) override;
+
+ private:
+  int mNumNodeFeatures = 8;
+};
+
+class QOI3D : public QOI {
+ public:
+  explicit QOI3D(const QoiGrid& g);
+  void searchJunctionsOnImage(const QoiGrid& g, const int* alpha) override;
+
+ private:
+  int mNumNodeFeatures = 9;
+};
+
+}  // namespace cupf_host

@@ -1,0 +1,103 @@
+"""ctypes binding of include/cupf_host.h (host side of the APT driver)."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+
+_FP = C.POINTER(C.c_float)
+_IP = C.POINTER(C.c_int32)
+
+_bound = False
+
+
+def _lib():
+    global _bound
+    L = abi.lib()
+    if not _bound:
+        L.cupf_host_grain_volumes.argtypes = [C.c_int] * 3 + [_IP, _IP, _IP, C.c_int]
+        L.cupf_host_line_qois.argtypes = [C.c_int] * 4 + [_IP, _IP, _IP, C.c_int, _IP, _IP, _IP]
+        L.cupf_host_sample_heights.argtypes = [_IP, _IP, C.c_int, C.c_int, C.c_int]
+        L.cupf_host_junctions_3d.argtypes = [C.c_int] * 3 + [_IP, _IP, C.c_int]
+        L.cupf_host_get_param_float.argtypes = [C.c_char_p, C.c_char_p, _FP]
+        L.cupf_host_get_param_int.argtypes = [C.c_char_p, C.c_char_p, _IP]
+        L.cupf_host_get_options.argtypes = [C.c_int, C.POINTER(C.c_char_p), _IP, C.c_char_p,
+                                            C.c_char_p, C.c_char_p, C.c_int]
+        L.cupf_host_setup.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                      _IP, _FP, _FP, _IP, C.c_int64, C.c_char_p, C.c_int]
+        _bound = True
+    return L
+
+
+def _i(a):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_IP)
+
+
+def grain_volumes(fnx, fny, fnz, alpha, cap=1 << 20):
+    g = np.zeros(cap, np.int32)
+    v = np.zeros(cap, np.int32)
+    n = _lib().cupf_host_grain_volumes(fnx, fny, fnz, _i(alpha), _i(g), _i(v), cap)
+    if n < 0:
+        raise ValueError("too many grains")
+    return g[:n].copy(), v[:n].copy()
+
+
+def line_qois(fnx, fny, fnz, num_theta, cur_tip, alpha, loss_area, move_count):
+    tip = C.c_int(cur_tip)
+    tip_y = np.zeros(1, np.int32)
+    tot = np.zeros(num_theta, np.int32)
+    ext = np.zeros(num_theta, np.int32)
+    _lib().cupf_host_line_qois(fnx, fny, fnz, num_theta, C.byref(tip), _i(alpha), _i(loss_area),
+                               move_count, _i(tip_y), _i(tot), _i(ext))
+    return tip.value, int(tip_y[0]), tot, ext
+
+
+def sample_heights(cur_tip, alpha, fnx, fny, fnz):
+    t = np.array([cur_tip], np.int32)
+    _lib().cupf_host_sample_heights(_i(t), _i(alpha), fnx, fny, fnz)
+    return int(t[0])
+
+
+def junctions_3d(fnx, fny, fnz, alpha, cap=1 << 22):
+    out = np.zeros(cap, np.int32)
+    n = _lib().cupf_host_junctions_3d(fnx, fny, fnz, _i(alpha), _i(out), cap)
+    return out[:n].copy()
+
+
+def get_param(line, key, kind=float, init=0):
+    if kind is float:
+        v = C.c_float(init)
+        _lib().cupf_host_get_param_float(line.encode(), key.encode(), C.byref(v))
+    else:
+        v = C.c_int32(init)
+        _lib().cupf_host_get_param_int(line.encode(), key.encode(), C.byref(v))
+    return v.value
+
+
+def get_options(argv):
+    arr = (C.c_char_p * len(argv))(*[a.encode() for a in argv])
+    out = np.zeros(10, np.int32)
+    b1, b2, b3 = (C.create_string_buffer(512) for _ in range(3))
+    _lib().cupf_host_get_options(len(argv), arr, _i(out), b1, b2, b3, 511)
+    return out, b1.value.decode(), b2.value.decode(), b3.value.decode()
+
+
+def setup(input_file, folder, bc=(0, 0, 0), line_config=False, pure_nucleation=False,
+          length_cap=1 << 26):
+    """parseInputParams + cpuSetup + initField; returns (dims, fparams, phi, alpha)."""
+    dims = np.zeros(4, np.int32)
+    fp = np.zeros(8, np.float32)
+    phi = np.zeros(length_cap, np.float32)
+    alpha = np.zeros(length_cap, np.int32)
+    err = C.create_string_buffer(512)
+    flags = (1 if line_config else 0) | (2 if pure_nucleation else 0)
+    r = _lib().cupf_host_setup(input_file.encode(), folder.encode(), bc[0], bc[1], bc[2], flags,
+                               _i(dims), fp.ctypes.data_as(_FP), phi.ctypes.data_as(_FP),
+                               _i(alpha), length_cap, err, 511)
+    if r != 0:
+        raise RuntimeError(err.value.decode())
+    L = int(dims[0]) * int(dims[1]) * int(dims[2])
+    return dims, fp, phi[:L].copy(), alpha[:L].copy()

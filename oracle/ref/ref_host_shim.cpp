@@ -51,6 +51,20 @@ int refq_calculate_line_qois(int fnx, int fny, int fnz, int num_theta, int nts, 
   return 0;
 }
 
+// QOI3D::searchJunctionsOnImage (QOI.cpp:233-311) after calculateQoIs.
+int refq_junctions_3d(int fnx, int fny, int fnz, const int* alpha, int* nodes, int cap) {
+  GlobalConstants p;
+  std::memset(&p, 0, sizeof(p));
+  p.fnx = fnx; p.fny = fny; p.fnz = fnz;
+  QOI3D q(p);
+  q.calculateQoIs(p, alpha, 0);
+  q.searchJunctionsOnImage(p, alpha);
+  const std::vector<int>& v = q.mQoIVectorIntData["node_region"];
+  const int n = (int)v.size();
+  for (int i = 0; i < n && i < cap; ++i) nodes[i] = v[i];
+  return n;
+}
+
 // QOI::sampleHeights (QOI.cpp:162-185).
 int refq_sample_heights(int* cur_tip, const int* alpha, int fnx, int fny, int fnz) {
   GlobalConstants p;
