@@ -202,6 +202,76 @@ def run_reference(args, ws, rank):
     return 0
 
 
+SERVE_GRIDS = [(48, 48, 48), (96, 96, 96), (128, 128, 256), (192, 192, 192)]
+
+
+def serve_requests(n, seed=0):
+    """Seeded config-4 stream: grid uniform from SERVE_GRIDS, 10-300 grains,
+    seed 0-9999, G 0.1-10 K/um (1e5-1e7 K/m), R 0.01-0.5 m/s, 1000 steps,
+    Poisson arrivals at 4 per second."""
+    from cupf_b200 import cases
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for _ in range(n):
+        t += rng.exponential(1.0 / 4.0)
+        g = SERVE_GRIDS[rng.integers(len(SERVE_GRIDS))]
+        c = cases.line_case(*g, num_pf=NUM_PF, num_grains=int(rng.integers(10, 301)),
+                            seed=int(rng.integers(0, 10000)), G=float(rng.uniform(0.1, 10.0)),
+                            R=float(rng.uniform(0.01, 0.5)), bc="110")
+        out.append((t, c))
+    return out
+
+
+def run_serve(args):
+    """Continuous-batching benchmark: submit each request at its arrival time,
+    pump the server meanwhile; report sims/hr and p50/p99 time-to-result."""
+    import torch
+    from cupf_b200.server import Server
+    torch.cuda.set_device(0)
+    reqs = serve_requests(args.serve_requests)
+    lines = []
+    for prec in args.serve_precisions.split(","):
+        with Server(precision=prec, num_pf=NUM_PF, max_active=64, steps_per_round=25,
+                    autotune=True) as srv:
+            # warm the autotuner and the kernels on one request of every grid shape
+            warm = [srv.submit(c, 5) for c in
+                    [next(c for _, c in reqs if c.meta["interior"] == g) for g in SERVE_GRIDS
+                     if any(c.meta["interior"] == g for _, c in reqs)]]
+            srv.run_until_done(warm)
+            for w in warm:
+                srv.release(w)
+            t0 = time.perf_counter()
+            ids = []
+            cells = 0
+            k = 0
+            with ClockSampler(0) as clk:
+                while k < len(reqs) or any(srv.status(r) < 2 for r in ids):
+                    now = time.perf_counter() - t0
+                    while k < len(reqs) and reqs[k][0] <= now:
+                        c = reqs[k][1]
+                        ids.append(srv.submit(c, CONFIG_STEPS))
+                        p = c.params
+                        cells += (p.fnx - 2) * (p.fny - 2) * (p.fnz - 2) * CONFIG_STEPS
+                        k += 1
+                    running, pending, _ = srv.pump()
+                    if running == 0 and pending == 0 and k < len(reqs):
+                        time.sleep(max(0.0, reqs[k][0] - (time.perf_counter() - t0)))
+            res = [srv.result(r) for r in ids]
+            ttr = np.array([r["times"][2] - r["times"][0] for r in res])
+            span = max(r["times"][2] for r in res) - min(r["times"][0] for r in res)
+            lines.append({"metric": "served sims/hr", "impl": "cupf-serve", "precision": prec,
+                          "value": len(res) / span * 3600.0, "unit": "sims/hr",
+                          "p50_s": float(np.percentile(ttr, 50)),
+                          "p99_s": float(np.percentile(ttr, 99)),
+                          "mcell_upd_per_s": cells / span / 1e6, "requests": len(res),
+                          "arrival_rate_per_s": 4.0, "steps_per_request": CONFIG_STEPS,
+                          "grids": [list(g) for g in SERVE_GRIDS], "clocks": clk.summary(),
+                          "data": "synthetic Poisson stream, seed 0"})
+            print(json.dumps(lines[-1]), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -210,11 +280,17 @@ def main():
     ap.add_argument("--impl", default="cupf", choices=["cupf", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--serve", action="store_true", help="served-batch benchmark (config 4)")
+    ap.add_argument("--serve-requests", type=int, default=40)
+    ap.add_argument("--serve-precisions", default="fp32,fp16")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp16"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local = dist_env()
     if args.impl == "reference":
         return run_reference(args, ws, rank)
+    if args.serve:
+        return run_serve(args)
 
     import torch
     from cupf_b200.solver import APTSolver

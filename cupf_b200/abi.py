@@ -43,6 +43,12 @@ class cupf_apt_inputs(C.Structure):
                                   "t_mac", "psi_mac", "T_3D")]
 
 
+class cupf_server_config(C.Structure):
+    _fields_ = [("device", C.c_int32), ("precision", C.c_int32), ("num_pf", C.c_int32),
+                ("max_active", C.c_int32), ("steps_per_round", C.c_int32),
+                ("autotune", C.c_int32), ("hbm_budget_bytes", C.c_int64)]
+
+
 STATUS = {0: "CUPF_OK", 1: "CUPF_ERR_INVALID", 2: "CUPF_ERR_CUDA", 3: "CUPF_ERR_OOM",
           4: "CUPF_ERR_UNSUPPORTED", 5: "CUPF_ERR_TIMEOUT", 6: "CUPF_ERR_IO", 7: "CUPF_ERR_STATE"}
 
@@ -81,12 +87,24 @@ def lib():
             "cupf_apt_steps_done": [vp, C.POINTER(C.c_int64)],
             "cupf_apt_collect": [vp, C.c_int32, FP, C.POINTER(C.c_int32)],
             "cupf_apt_grain_volumes": [vp, C.c_int32, C.POINTER(C.c_int64)],
+            "cupf_apt_qoi_sums": [vp, C.POINTER(C.c_double)],
             "cupf_apt_move_domain": [vp, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32),
                                      C.POINTER(C.c_int32)],
             "cupf_apt_get_archive": [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)],
             "cupf_apt_get_z": [vp, FP],
             "cupf_apt_sync": [vp, C.c_int32],
             "cupf_apt_time_steps": [vp, C.c_int32, FP],
+            "cupf_apt_set_tuning": [vp, C.c_int32],
+            "cupf_server_create": [C.POINTER(cupf_server_config), C.POINTER(vp)],
+            "cupf_server_destroy": [vp],
+            "cupf_server_submit": [vp, C.POINTER(cupf_apt_params), C.POINTER(cupf_apt_inputs), FP,
+                                   C.POINTER(C.c_int32), C.c_int64, C.POINTER(C.c_int64)],
+            "cupf_server_pump": [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                 C.POINTER(C.c_int32)],
+            "cupf_server_result": [vp, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                   C.POINTER(C.c_int64), C.c_int32, C.POINTER(C.c_double),
+                                   C.POINTER(C.c_double)],
+            "cupf_server_release": [vp, C.c_int64],
         }.items():
             f = getattr(L, name)
             f.argtypes = args

@@ -5,7 +5,7 @@
 // events and on read-back.
 #pragma once
 
-#include "apt_common.cuh"
+#include "apt_storage.cuh"
 
 namespace cupf {
 
@@ -19,15 +19,12 @@ struct Grid {
   __host__ __device__ long long length() const { return (long long)fnx * fny * fnz; }
 };
 
-__device__ __forceinline__ uint2 empty_pair() {
-  return make_uint2(__float_as_uint(-1.0f), 0xFFFFFFFFu);
-}
-
 // Materialise the halo: every cell with a coordinate on the boundary takes the
 // record of its mapped interior source (each coordinate mapped independently,
 // = sequential z, y, x face fills of APTsetBC3D, APTPhaseField.cu:93-174).
 // Cells are enumerated face by face without repetition.
-__global__ void fill_halo_kernel(uint2* buf, Grid g, int bcX, int bcY, int bcZ) {
+template <class S>
+__global__ void fill_halo_kernel(typename S::T* buf, Grid g, int bcX, int bcY, int bcZ) {
   const long long nz2 = 2ll * g.fnx * g.fny;
   const long long ny2 = 2ll * g.fnx * (g.fnz - 2);
   const long long nx2 = 2ll * (g.fny - 2) * (g.fnz - 2);
@@ -61,7 +58,8 @@ __global__ void fill_halo_kernel(uint2* buf, Grid g, int bcX, int bcY, int bcZ) 
 // set_minus1 + APTini_PF on both buffers (PhaseField.cu:51-57, APTPhaseField.cu:78-89):
 // every slot (-1, -1), then slot 0 = (phi, alpha) where phi > LS.  phi/alpha in
 // reference layout (index i + j*fnx + k*fnx*fny).
-__global__ void init_kernel(uint2* A, uint2* B, const float* __restrict__ phi,
+template <class S>
+__global__ void init_kernel(typename S::T* A, typename S::T* B, const float* __restrict__ phi,
                             const int* __restrict__ alpha, Grid g) {
   const long long L = g.length();
   for (long long C = blockIdx.x * (long long)blockDim.x + threadIdx.x; C < L;
@@ -71,20 +69,22 @@ __global__ void init_kernel(uint2* A, uint2* B, const float* __restrict__ phi,
     const int k = (int)(C / ((long long)g.fnx * g.fny));
     const long long d = g.at(i, j, k);
     const float v = phi[C];
-    uint2 s0 = empty_pair();
-    if ((double)v > LS) s0 = make_uint2(__float_as_uint(v), (uint32_t)alpha[C]);
+    typename S::T s0 = S::empty();
+    if ((double)v > LS) s0 = S::make(v, alpha[C]);
     A[d] = s0;
     B[d] = s0;
     for (int p = 1; p < g.np; ++p) {
-      A[p * g.ss + d] = empty_pair();
-      B[p * g.ss + d] = empty_pair();
+      A[p * g.ss + d] = S::empty();
+      B[p * g.ss + d] = S::empty();
     }
   }
 }
 
 // APTcollect_PF (APTPhaseField.cu:55-75): argmax over slots, first max wins; the
 // outputs change only where the max is above LS.
-__global__ void collect_kernel(const uint2* __restrict__ buf, float* phi, int* alpha, Grid g) {
+template <class S>
+__global__ void collect_kernel(const typename S::T* __restrict__ buf, float* phi, int* alpha,
+                               Grid g) {
   const long long L = g.length();
   for (long long C = blockIdx.x * (long long)blockDim.x + threadIdx.x; C < L;
        C += (long long)gridDim.x * blockDim.x) {
@@ -92,20 +92,26 @@ __global__ void collect_kernel(const uint2* __restrict__ buf, float* phi, int* a
     const int j = (int)((C / g.fnx) % g.fny);
     const int k = (int)(C / ((long long)g.fnx * g.fny));
     const long long d = g.at(i, j, k);
-    uint2 best = buf[d];
+    typename S::T best = buf[d];
+    float bv = S::phi(best);
     for (int p = 1; p < g.np; ++p) {
-      const uint2 v = buf[p * g.ss + d];
-      if (__uint_as_float(v.x) > __uint_as_float(best.x)) best = v;
+      const typename S::T v = buf[p * g.ss + d];
+      const float f = S::phi(v);
+      if (f > bv) {
+        best = v;
+        bv = f;
+      }
     }
-    if ((double)__uint_as_float(best.x) > LS) {
-      phi[C] = __uint_as_float(best.x);
-      alpha[C] = (int)best.y;
+    if ((double)bv > LS) {
+      phi[C] = bv;
+      alpha[C] = S::id(best);
     }
   }
 }
 
 // pair planes -> reference layout (ph[slot*length + C], ids[slot*length + C])
-__global__ void export_kernel(const uint2* __restrict__ buf, float* ph, int* ids, Grid g) {
+template <class S>
+__global__ void export_kernel(const typename S::T* __restrict__ buf, float* ph, int* ids, Grid g) {
   const long long L = g.length();
   for (long long C = blockIdx.x * (long long)blockDim.x + threadIdx.x; C < L * g.np;
        C += (long long)gridDim.x * blockDim.x) {
@@ -114,14 +120,15 @@ __global__ void export_kernel(const uint2* __restrict__ buf, float* ph, int* ids
     const int i = (int)(c % g.fnx);
     const int j = (int)((c / g.fnx) % g.fny);
     const int k = (int)(c / ((long long)g.fnx * g.fny));
-    const uint2 v = buf[p * g.ss + g.at(i, j, k)];
-    ph[C] = __uint_as_float(v.x);
-    ids[C] = (int)v.y;
+    const typename S::T v = buf[p * g.ss + g.at(i, j, k)];
+    ph[C] = S::phi(v);
+    ids[C] = S::id(v);
   }
 }
 
-__global__ void import_kernel(uint2* buf, const float* __restrict__ ph, const int* __restrict__ ids,
-                              Grid g) {
+template <class S>
+__global__ void import_kernel(typename S::T* buf, const float* __restrict__ ph,
+                              const int* __restrict__ ids, Grid g) {
   const long long L = g.length();
   for (long long C = blockIdx.x * (long long)blockDim.x + threadIdx.x; C < L * g.np;
        C += (long long)gridDim.x * blockDim.x) {
@@ -130,21 +137,22 @@ __global__ void import_kernel(uint2* buf, const float* __restrict__ ph, const in
     const int i = (int)(c % g.fnx);
     const int j = (int)((c / g.fnx) % g.fny);
     const int k = (int)(c / ((long long)g.fnx * g.fny));
-    buf[p * g.ss + g.at(i, j, k)] = make_uint2(__float_as_uint(ph[C]), (uint32_t)ids[C]);
+    buf[p * g.ss + g.at(i, j, k)] = S::make(ph[C], ids[C]);
   }
 }
 
 // Per-layer sum of phi over every slot and cell (halo included), one block per
 // layer, double accumulation in a fixed order (deterministic; the reference
 // accumulates with float atomics, PhaseField.cu:366-378).
-__global__ void layer_sum_kernel(const uint2* __restrict__ buf, double* sums, Grid g) {
+template <class S>
+__global__ void layer_sum_kernel(const typename S::T* __restrict__ buf, double* sums, Grid g) {
   const int k = blockIdx.x;
   double acc = 0.0;
   const long long n = (long long)g.fnx * g.fny;
   for (int p = 0; p < g.np; ++p)
     for (long long c = threadIdx.x; c < n; c += blockDim.x) {
       const int i = (int)(c % g.fnx), j = (int)(c / g.fnx);
-      acc += (double)__uint_as_float(buf[p * g.ss + g.at(i, j, k)].x);
+      acc += (double)S::phi(buf[p * g.ss + g.at(i, j, k)]);
     }
   __shared__ double red[256];
   red[threadIdx.x] = acc;
@@ -159,7 +167,8 @@ __global__ void layer_sum_kernel(const uint2* __restrict__ buf, double* sums, Gr
 // One-layer shift of the interior (APTmove_frame + APTcopy_frame,
 // APTPhaseField.cu:357-410): dst[k] = src[k+1] for k < fnz-2, top interior layer
 // (-1, -1).  Halo cells are not touched.
-__global__ void shift_kernel(const uint2* __restrict__ src, uint2* dst, Grid g) {
+template <class S>
+__global__ void shift_kernel(const typename S::T* __restrict__ src, typename S::T* dst, Grid g) {
   const int ni = g.fnx - 2, nj = g.fny - 2, nk = g.fnz - 2;
   const long long total = (long long)ni * nj * nk * g.np;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
@@ -172,11 +181,13 @@ __global__ void shift_kernel(const uint2* __restrict__ src, uint2* dst, Grid g) 
     const int k = 1 + (int)(r % nk);
     const int p = (int)(r / nk);
     const long long d = p * g.ss + g.at(i, j, k);
-    dst[d] = (k < g.fnz - 2) ? src[p * g.ss + g.at(i, j, k + 1)] : empty_pair();
+    dst[d] = (k < g.fnz - 2) ? src[p * g.ss + g.at(i, j, k + 1)] : S::empty();
   }
 }
 
-__global__ void copy_interior_kernel(const uint2* __restrict__ src, uint2* dst, Grid g) {
+template <class S>
+__global__ void copy_interior_kernel(const typename S::T* __restrict__ src, typename S::T* dst,
+                                     Grid g) {
   const int ni = g.fnx - 2, nj = g.fny - 2, nk = g.fnz - 2;
   const long long total = (long long)ni * nj * nk * g.np;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
@@ -196,7 +207,7 @@ __global__ void copy_interior_kernel(const uint2* __restrict__ src, uint2* dst, 
 // Archive the bottom interior layer of the argmax map and count it into the
 // lost area (APTPhaseField.cu:383-388): alpha_full[move*plane + C] = alpha[C] for
 // C in layer 1 (all i, j), loss_area[alpha-1] += 1 for alpha in 1..num_theta.
-__global__ void archive_kernel(const int* __restrict__ alpha, int* alpha_full, int* loss_area,
+static __global__ void archive_kernel(const int* __restrict__ alpha, int* alpha_full, int* loss_area,
                                int fnx, int fny, int move_count, int num_theta) {
   const long long plane = (long long)fnx * fny;
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < plane;
@@ -210,7 +221,7 @@ __global__ void archive_kernel(const int* __restrict__ alpha, int* alpha_full, i
 // Voxel count per grain id over the interior of the argmax map, plus the first
 // (k, j, i)-order index where each id occurs (for the reference's first-seen
 // ordering, QOI.cpp:198-231).  counts[0] = interior cells with no grain.
-__global__ void volume_kernel(const int* __restrict__ alpha, int fnx, int fny, int fnz, int ng,
+static __global__ void volume_kernel(const int* __restrict__ alpha, int fnx, int fny, int fnz, int ng,
                               unsigned long long* counts, long long* first) {
   const long long ni = fnx - 2, nj = fny - 2, nk = fnz - 2;
   const long long total = ni * nj * nk;
@@ -225,6 +236,54 @@ __global__ void volume_kernel(const int* __restrict__ alpha, int fnx, int fny, i
     } else {
       atomicAdd(counts, 1ull);
     }
+  }
+}
+
+// FP64 interface QoIs over the interior, from m = max-over-slots phi of each cell:
+//   part[2*b]   = sum (1 + m) / 2              (solid volume, cell units)
+//   part[2*b+1] = sum |grad m| / 2             (interface area, cell units; a
+//                 diffuse interface integrates |grad phi| to 2 across its width)
+// with central differences of m on the 6 neighbours (halo cells filled first).
+// One partial pair per block; the host adds the partials in block order.
+template <class S>
+__device__ __forceinline__ float max_phi(const typename S::T* __restrict__ buf, const Grid& g,
+                                         long long d) {
+  float m = S::phi(buf[d]);
+  for (int p = 1; p < g.np; ++p) m = fmaxf(m, S::phi(buf[p * g.ss + d]));
+  return m;
+}
+
+template <class S>
+__global__ void qoi_sums_kernel(const typename S::T* __restrict__ buf, Grid g, double* part) {
+  const long long ni = g.fnx - 2, nj = g.fny - 2, nk = g.fnz - 2;
+  const long long total = ni * nj * nk;
+  double vol = 0.0, area = 0.0;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int i = 1 + (int)(idx % ni), j = 1 + (int)((idx / ni) % nj), k = 1 + (int)(idx / (ni * nj));
+    const long long d = g.at(i, j, k);
+    const double m = max_phi<S>(buf, g, d);
+    vol += 0.5 * (1.0 + m);
+    const double gx = 0.5 * ((double)max_phi<S>(buf, g, d + 1) - max_phi<S>(buf, g, d - 1));
+    const double gy = 0.5 * ((double)max_phi<S>(buf, g, d + g.xp) - max_phi<S>(buf, g, d - g.xp));
+    const double gz =
+        0.5 * ((double)max_phi<S>(buf, g, d + g.plane()) - max_phi<S>(buf, g, d - g.plane()));
+    area += 0.5 * sqrt(gx * gx + gy * gy + gz * gz);
+  }
+  __shared__ double rv[256], ra[256];
+  rv[threadIdx.x] = vol;
+  ra[threadIdx.x] = area;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+      rv[threadIdx.x] += rv[threadIdx.x + s];
+      ra[threadIdx.x] += ra[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = rv[0];
+    part[2 * blockIdx.x + 1] = ra[0];
   }
 }
 

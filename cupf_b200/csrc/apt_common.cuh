@@ -18,6 +18,12 @@ namespace cupf {
 
 constexpr double LS = -0.995;     // liquid threshold (APTPhaseField.cu:25)
 constexpr double ID_DROP = -0.9999; // id is dropped below this phi (:341)
+// The reference compares float phi with these double literals.  For a float f,
+//   (double)f > -0.995  <=>  f > 0xbf7eb852 (-0.99500000477...)  (largest float <= -0.995)
+//   (double)f < -0.9999 <=>  f < 0xbf7ff972 (-0.99989998340...)  (smallest float >= -0.9999)
+// so the kernels compare in single precision with these bit patterns.
+constexpr uint32_t kLSFloatBits = 0xbf7eb852u;
+constexpr uint32_t kDropFloatBits = 0xbf7ff972u;
 
 // Per-launch arguments of the step kernel (passed by value).
 struct StepArgs {
@@ -27,7 +33,7 @@ struct StepArgs {
   int ntx, nty, nzc, zc;  // tile grid and z-chunk length
   int num_theta, thermalType, use_iuc;
   float t;
-  float kin_delta, eps, G, z0, uc, uc0, L_cp, hi, lamd, dt;
+  float kin_delta, eps, G, z0, uc, uc0, L_cp, hi, lamd, dt, tau0;
   float lyd, lzd, r0, x0, angle, V, mp_len, order;
   int Nx, Ny, Nz;
   const float* x;
@@ -39,9 +45,10 @@ struct StepArgs {
   const float* Y_mac;
   const float* Z_mac;
   const float* psi_mac;
-  const uint2* in;   // pair buffer read this step
-  uint2* out;        // pair buffer written this step
+  const void* in;    // pair buffer read this step (storage format of the launch)
+  void* out;         // pair buffer written this step
   int* err;          // device error word (0 = ok)
+  int* work;         // [next item, CTAs done] of the persistent launch (self-resetting)
 };
 
 // Boundary map of one coordinate (APTsetBC3D, APTPhaseField.cu:111-112,134-135,157-158):

@@ -27,6 +27,7 @@
 // merge overflow (local_phs[s][NUM_PF] == local_phs[s+1][0]).
 #pragma once
 
+#include "apt_storage.cuh"
 #include "apt_update.cuh"
 
 namespace cupf {
@@ -34,16 +35,16 @@ namespace cupf {
 constexpr int TX = 32;
 constexpr int TY = 8;
 constexpr int NTHREADS = TX * TY;
-constexpr int BW = TX + 2;  // box width (cells)
-constexpr int BH = TY + 2;  // box height
-constexpr int BCELLS = BW * BH;
+constexpr int BH = TY + 2;  // box height (cells); the box width is the storage format's kBW
 constexpr int STAGES = 5;
 
-template <int NP>
+template <int NP, class S>
 struct StepSmem {
-  static constexpr int kBoxBytes = NP * BCELLS * 8;                // bytes one TMA plane load delivers
+  static constexpr int BW = S::kBW;
+  static constexpr int BCELLS = BW * BH;
+  static constexpr int kBoxBytes = NP * BCELLS * S::kBytes;      // bytes one TMA plane load delivers
   static constexpr int kStageBytes = (kBoxBytes + 127) & ~127;  // stage stride (TMA dst: 128 B aligned)
-  static constexpr int kStagePairs = kStageBytes / 8;
+  static constexpr int kStagePairs = kStageBytes / S::kBytes;
   static constexpr int kMaskOff = STAGES * kStageBytes;
   static constexpr int kBarOff = (kMaskOff + STAGES * BCELLS * 2 + 7) & ~7;
   static constexpr int kBytes = kBarOff + STAGES * 8 + 16;  // + abort word, issued count
@@ -103,25 +104,68 @@ __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-template <int NP>
-__global__ void __launch_bounds__(NTHREADS, 2)
-    apt_step_kernel(const __grid_constant__ CUtensorMap tmap, const StepArgs a) {
+// Per-CTA shared-memory state, carved from the dynamic allocation.
+template <int NP, class S>
+struct CtaSmem {
+  using P = typename S::T;
+  using Smem = StepSmem<NP, S>;
+  P* stages;
+  uint16_t* masks;
+  uint64_t* bars;
+  int* s_abort;   // global plane sequence number of the first failed wait, + 1
+  int* s_issued;  // plane sequence numbers issued so far (written by thread 0)
+  int* s_item;    // work item handed to the CTA (batched kernel)
+  __device__ explicit CtaSmem(unsigned char* smem) {
+    stages = reinterpret_cast<P*>(smem);
+    masks = reinterpret_cast<uint16_t*>(smem + Smem::kMaskOff);
+    bars = reinterpret_cast<uint64_t*>(smem + Smem::kBarOff);
+    s_abort = reinterpret_cast<int*>(smem + Smem::kBarOff + STAGES * 8);
+    s_issued = s_abort + 1;
+    s_item = s_abort + 2;
+  }
+  __device__ void init() {
+    if (threadIdx.x == 0) {
+      for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
+      *s_abort = 0;
+      *s_issued = 0;
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+  }
+  // After a timed-out wait no further loads are issued; before the CTA exits
+  // (and its shared memory is reused) wait, again bounded, for those in flight.
+  __device__ void drain() {
+    __syncthreads();
+    if (threadIdx.x == 0 && *s_abort) {
+      for (int q = *s_abort - 1; q < *s_issued; ++q)
+        mbar_wait_bounded(&bars[q % STAGES], (uint32_t)((q / STAGES) & 1));
+    }
+  }
+};
+
+// One work item: the column tile (txi, tyi) over the z chunk zci of one
+// simulation.  qbase is the CTA's running plane sequence number: plane q of
+// this item is sequence number qbase + q, which fixes its stage (mod STAGES)
+// and the mbarrier phase parity; every issued plane is waited exactly once, in
+// order, so the phases stay consistent across items.
+template <int NP, class S>
+__device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArgs& a, int txi,
+                                          int tyi, int zci, CtaSmem<NP, S>& sm, int& qbase) {
   using Map = CodeMap<NP>;
-  using Smem = StepSmem<NP>;
-  extern __shared__ __align__(128) unsigned char smem[];
-  uint2* stages = reinterpret_cast<uint2*>(smem);
-  uint16_t* masks = reinterpret_cast<uint16_t*>(smem + Smem::kMaskOff);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Smem::kBarOff);
-  int* s_abort = reinterpret_cast<int*>(smem + Smem::kBarOff + STAGES * 8);  // first failed plane + 1
-  int* s_issued = s_abort + 1;  // planes issued so far (written by thread 0)
+  using Smem = StepSmem<NP, S>;
+  using P = typename S::T;
+  constexpr int BW = Smem::BW;
+  constexpr int BCELLS = Smem::BCELLS;
+  P* stages = sm.stages;
+  uint16_t* masks = sm.masks;
+  uint64_t* bars = sm.bars;
+  int* s_abort = sm.s_abort;
+  int* s_issued = sm.s_issued;
+  const P* gin = static_cast<const P*>(a.in);
+  P* gout = static_cast<P*>(a.out);
 
   const int tid = threadIdx.x;
   const int tx = tid % TX, ty = tid / TX;
-  int b = blockIdx.x;
-  const int zci = b % a.nzc;
-  b /= a.nzc;
-  const int txi = b % a.ntx;
-  const int tyi = b / a.ntx;
   const int x0 = 1 + TX * txi;  // first interior x of the tile
   const int y0 = 1 + TY * tyi;
   const int k_begin = 1 + a.zc * zci;
@@ -129,25 +173,22 @@ __global__ void __launch_bounds__(NTHREADS, 2)
   const int nplanes = k_end - k_begin + 2;  // planes k_begin-1 .. k_end
   const long long ss = a.slot_stride;
   const long long plane_pairs = (long long)a.xp * a.fny;
-
-  if (tid == 0) {
-    for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
-    *s_abort = 0;
-    *s_issued = 0;
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
+  const int q0 = qbase;
 
   auto issue = [&](int q) {  // plane index q -> logical z = k_begin - 1 + q
-    const int s = q % STAGES;
+    const int g = q0 + q;
+    const int s = g % STAGES;
     const int zl = k_begin - 1 + q;
     const int zp = bc_map(zl, a.fnz, a.bcZ);
     mbar_arrive_expect_tx(&bars[s], Smem::kBoxBytes);
-    tma_load_plane(stages + (size_t)s * Smem::kStagePairs, &tmap, &bars[s], x0 - 1, y0 - 1, zp);
-    *s_issued = q + 1;
+    tma_load_plane(stages + (size_t)s * Smem::kStagePairs, tmap, &bars[s], x0 - 1, y0 - 1, zp);
+    *s_issued = g + 1;
   };
 
-  if (tid == 0) {
+  // the previous item (if any) is done with every stage before they refill
+  __syncthreads();
+  if (tid == 0 && !*s_abort) {
+    fence_proxy_async();
     const int npre = min(STAGES, nplanes);
     for (int q = 0; q < npre; ++q) issue(q);
   }
@@ -155,15 +196,17 @@ __global__ void __launch_bounds__(NTHREADS, 2)
   // Wait for plane q, patch its x/y halo cells from their mapped sources, and
   // compute the occupancy masks of its cells (same thread per cell for both).
   auto land = [&](int q) {
-    const int s = q % STAGES;
-    const uint32_t parity = (uint32_t)((q / STAGES) & 1);
+    const int g = q0 + q;
+    const int s = g % STAGES;
+    const uint32_t parity = (uint32_t)((g / STAGES) & 1);
     if (!*s_abort) {
-      if (!mbar_wait_bounded(&bars[s], parity)) {
-        atomicCAS(s_abort, 0, q + 1);
+      // another CTA already gave up: do not spend a second per CTA finding out again
+      if (*(volatile int*)a.err != 0 || !mbar_wait_bounded(&bars[s], parity)) {
+        atomicCAS(s_abort, 0, g + 1);
         atomicExch(a.err, ERR_TMA_TIMEOUT);
       }
     }
-    uint2* st = stages + (size_t)s * Smem::kStagePairs;
+    P* st = stages + (size_t)s * Smem::kStagePairs;
     const int zl = k_begin - 1 + q;
     const int zp = bc_map(zl, a.fnz, a.bcZ);
     for (int c = tid; c < BCELLS; c += NTHREADS) {
@@ -174,11 +217,11 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         const int mx = bc_map(gx, a.fnx, a.bcX), my = bc_map(gy, a.fny, a.bcY);
         const long long src = (long long)zp * plane_pairs + (long long)my * a.xp + mx;
 #pragma unroll
-        for (int p = 0; p < NP; ++p) st[p * BCELLS + c] = __ldg(a.in + p * ss + src);
+        for (int p = 0; p < NP; ++p) st[p * BCELLS + c] = gin[p * ss + src];
       }
       uint32_t m = 0;
 #pragma unroll
-      for (int p = 0; p < NP; ++p) m |= (uint32_t)((int)st[p * BCELLS + c].y != -1) << p;
+      for (int p = 0; p < NP; ++p) m |= (uint32_t)(S::id(st[p * BCELLS + c]) != -1) << p;
       masks[s * BCELLS + c] = (uint16_t)m;
     }
   };
@@ -189,9 +232,20 @@ __global__ void __launch_bounds__(NTHREADS, 2)
   const int gx = x0 + tx, gy = y0 + ty;
   const bool valid = gx <= a.fnx - 2 && gy <= a.fny - 2;
   const int c = (ty + 1) * BW + (tx + 1);
+  // the line profile and the liquid-start undercooling depend on z only: one
+  // evaluation per plane instead of one per cell
+  const bool plane_T = a.use_iuc || a.thermalType == 0 || a.thermalType == 1;
+  const float kLS = __uint_as_float(kLSFloatBits);
+  const float kDrop = __uint_as_float(kDropFloatBits);
 
   for (int k = k_begin; k < k_end; ++k) {
     const int qk = k - k_begin + 1;
+    float Up_plane = 0.0f;
+    if (plane_T) {
+      float T;
+      tinterp(a, 0, 0, k, &T);
+      Up_plane = __fdiv_rn(T, a.L_cp);
+    }
     land(qk + 1);
     __syncthreads();
     if (tid == 0 && qk >= 2 && qk - 2 + STAGES < nplanes && !*s_abort) {
@@ -200,11 +254,11 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     }
     if (!valid) continue;
 
-    const int sD = (qk - 1) % STAGES, sC = qk % STAGES, sU = (qk + 1) % STAGES;
-    const uint2* pD = stages + (size_t)sD * Smem::kStagePairs + c;
-    const uint2* pC = stages + (size_t)sC * Smem::kStagePairs + c;
-    const uint2* pU = stages + (size_t)sU * Smem::kStagePairs + c;
-    const uint2* pts[7] = {pD, pC - BW, pC - 1, pC, pC + 1, pC + BW, pU};
+    const int sD = (q0 + qk - 1) % STAGES, sC = (q0 + qk) % STAGES, sU = (q0 + qk + 1) % STAGES;
+    const P* pD = stages + (size_t)sD * Smem::kStagePairs + c;
+    const P* pC = stages + (size_t)sC * Smem::kStagePairs + c;
+    const P* pU = stages + (size_t)sU * Smem::kStagePairs + c;
+    const P* pts[7] = {pD, pC - BW, pC - 1, pC, pC + 1, pC + BW, pU};
     uint32_t mk[7];
     mk[0] = masks[sD * BCELLS + c];
     mk[1] = masks[sC * BCELLS + c - BW];
@@ -214,10 +268,10 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     mk[5] = masks[sC * BCELLS + c + BW];
     mk[6] = masks[sU * BCELLS + c];
 
-    uint2* outp = a.out + (long long)k * plane_pairs + (long long)gy * a.xp + gx;
+    P* outp = gout + (long long)k * plane_pairs + (long long)gy * a.xp + gx;
     const uint32_t any = mk[0] | mk[1] | mk[2] | mk[3] | mk[4] | mk[5] | mk[6];
     if (any == 0) {
-      const uint2 empty = make_uint2(__float_as_uint(-1.0f), 0xFFFFFFFFu);
+      const P empty = S::empty();
 #pragma unroll
       for (int p = 0; p < NP; ++p) outp[p * ss] = empty;
       continue;
@@ -241,8 +295,8 @@ __global__ void __launch_bounds__(NTHREADS, 2)
       while (m) {
         const int p = __ffs(m) - 1;
         m &= m - 1;
-        const uint2 pr = pts[s][p * BCELLS];
-        const int id = (int)pr.y;
+        const P pr = pts[s][p * BCELLS];
+        const int id = S::id(pr);
         int j = n;
 #pragma unroll
         for (int q = NP - 1; q >= 0; --q)
@@ -257,7 +311,7 @@ __global__ void __launch_bounds__(NTHREADS, 2)
             // local_phs[s][NUM_PF] aliases local_phs[s+1][0]; past the array at s == 6
             if (s < 6) {
               code[s + 1] = (code[s + 1] & ~(Map)0xF) | (Map)0xE;
-              alias[s + 1] = __uint_as_float(pr.x);
+              alias[s + 1] = S::phi(pr);
             }
             continue;
           }
@@ -271,7 +325,7 @@ __global__ void __launch_bounds__(NTHREADS, 2)
       const uint32_t cd = (uint32_t)(code[s] >> (4 * j)) & 0xF;
       if (cd == 0xF) return -1.0f;
       if (cd == 0xE) return alias[s];
-      return __uint_as_float(pts[s][cd * BCELLS].x);
+      return S::phi(pts[s][cd * BCELLS]);
     };
 
     // center values of every slot (for the repulsion sum)
@@ -279,9 +333,9 @@ __global__ void __launch_bounds__(NTHREADS, 2)
 #pragma unroll
     for (int q = 0; q < NP; ++q) phc[q] = (q < n) ? fetch(3, q) : -1.0f;
 
-    float Up = 0.0f;
+    float Up = Up_plane;
     bool upd = true;
-    {
+    if (!plane_T) {
       float T;
       upd = tinterp(a, gx, gy, k, &T);
       Up = __fdiv_rn(T, a.L_cp);
@@ -289,44 +343,90 @@ __global__ void __launch_bounds__(NTHREADS, 2)
 
 #pragma unroll
     for (int j = 0; j < NP; ++j) {
-      uint2 o;
+      P o;
       if (j >= n) {
-        o = make_uint2(__float_as_uint(-1.0f), 0xFFFFFFFFu);
+        o = S::empty();
       } else if (!upd) {
         o = outp[j * ss];  // reference leaves the slot unwritten
       } else {
+        const int id = L[j];
+        // orientation of the grain (APTPhaseField.cu:259-273): loads issued before
+        // the stencil values are gathered so their latency overlaps; ids are >= 0
+        // here (cupf_apt_set_slots rejects other negative ids) and the clamp only
+        // keeps a corrupted id from reading outside the tables
+        int tid2 = id;
+        if (id > a.num_theta) tid2 = (id % a.num_theta) + 1;
+        const bool tab_ok = (unsigned)tid2 <= (unsigned)a.num_theta;
+        const int ti = tab_ok ? tid2 : 0;
+        const float t_sa = __ldg(a.sint + ti), t_ca = __ldg(a.cost + ti);
+        const float t_sb = __ldg(a.sint + ti + a.num_theta), t_cb = __ldg(a.cost + ti + a.num_theta);
         float ph7[7];
 #pragma unroll
         for (int s = 0; s < 7; ++s) ph7[s] = fetch(s, j);
-        const int id = L[j];
         float sina = 0.0f, cosa = 1.0f, sinb = 0.0f, cosb = 1.0f;
-        // ids are >= 0 here (cupf_apt_set_slots rejects other negative ids); the
-        // bound check only keeps a corrupted id from reading outside the tables
-        const int tid2 = id <= a.num_theta ? id : (id % a.num_theta) + 1;
-        if ((double)ph7[3] > LS && (unsigned)tid2 <= (unsigned)a.num_theta) {
-          sina = __ldg(a.sint + tid2);
-          cosa = __ldg(a.cost + tid2);
-          sinb = __ldg(a.sint + tid2 + a.num_theta);
-          cosb = __ldg(a.cost + tid2 + a.num_theta);
+        if (ph7[3] > kLS && tab_ok) {  // (double)phC > LS
+          sina = t_sa;
+          cosa = t_ca;
+          sinb = t_sb;
+          cosb = t_cb;
         }
         float repul = 0.0f;
 #pragma unroll
         for (int q = 0; q < NP; ++q)
           if (q != j && q < n) repul = repul_add(repul, phc[q]);
         const float nv = slot_update(a, ph7, sina, cosa, sinb, cosb, repul, Up);
-        o = make_uint2(__float_as_uint(nv), ((double)nv < ID_DROP) ? 0xFFFFFFFFu : (uint32_t)id);
+        o = S::make(nv, (nv < kDrop) ? -1 : id);  // (double)nv < -0.9999
       }
       outp[j * ss] = o;
     }
   }
 
-  // After a timed-out wait no further loads were issued; before the CTA exits
-  // (and its shared memory is reused) wait, again bounded, for those in flight.
-  __syncthreads();
-  if (tid == 0 && *s_abort) {
-    for (int q = *s_abort - 1; q < *s_issued; ++q)
-      mbar_wait_bounded(&bars[q % STAGES], (uint32_t)((q / STAGES) & 1));
+  qbase = q0 + nplanes;
+}
+
+// Hand the CTA its next work item from the launch's atomic counter (-1 when
+// none is left).  After its last fetch each CTA counts itself done; the last one
+// resets both words, so the next launch (or graph replay) starts from zero.
+__device__ __forceinline__ int next_work_item(int* work, int nitems, int* s_item) {
+  __syncthreads();  // every thread has read the previous index
+  if (threadIdx.x == 0) {
+    int it = atomicAdd(work, 1);
+    if (it >= nitems) {
+      it = -1;
+      __threadfence();
+      if (atomicAdd(work + 1, 1) == (int)gridDim.x - 1) {
+        atomicExch(work, 0);
+        atomicExch(work + 1, 0);
+      }
+    }
+    *s_item = it;
   }
+  __syncthreads();
+  return *s_item;
+}
+
+// One launch = one step of one simulation.  Persistent CTAs pull work items
+// (column tile x z chunk) from an atomic counter, z-chunk-major so the chunks
+// nearest the bottom (the solid, where cells carry the most grain ids in a
+// directional-solidification run) start first and the light liquid chunks fill
+// in behind them.
+template <int NP, class S>
+__global__ void __launch_bounds__(NTHREADS, 2)
+    apt_step_kernel(const __grid_constant__ CUtensorMap tmap, const StepArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  CtaSmem<NP, S> sm(smem);
+  sm.init();
+  const int per_chunk = a.ntx * a.nty;
+  const int nitems = per_chunk * a.nzc;
+  int qbase = 0;
+  for (;;) {
+    const int it = next_work_item(a.work, nitems, sm.s_item);
+    if (it < 0) break;
+    const int zci = it / per_chunk;
+    const int r = it - zci * per_chunk;
+    step_item<NP, S>(&tmap, a, r % a.ntx, r / a.ntx, zci, sm, qbase);
+  }
+  sm.drain();
 }
 
 }  // namespace cupf

@@ -7,6 +7,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
@@ -18,6 +19,7 @@
 
 #include "../../include/cupf.h"
 #include "apt_aux.cuh"
+#include "capi_internal.h"
 #include "apt_step.cuh"
 
 using namespace cupf;
@@ -25,7 +27,7 @@ using namespace cupf;
 // ------------------------------------------------------------------ errors
 static thread_local std::string g_err;
 
-static cupf_status fail(cupf_status st, const char* fmt, ...) {
+cupf_status cupf_fail(cupf_status st, const char* fmt, ...) {
   char buf[512];
   va_list ap;
   va_start(ap, fmt);
@@ -35,14 +37,7 @@ static cupf_status fail(cupf_status st, const char* fmt, ...) {
   return st;
 }
 
-#define CK(call)                                                                       \
-  do {                                                                                 \
-    cudaError_t e_ = (call);                                                           \
-    if (e_ != cudaSuccess)                                                             \
-      return fail(e_ == cudaErrorMemoryAllocation ? CUPF_ERR_OOM : CUPF_ERR_CUDA,      \
-                  "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__,   \
-                  __LINE__);                                                           \
-  } while (0)
+#define fail cupf_fail
 
 extern "C" const char* cupf_last_error(void) { return g_err.c_str(); }
 extern "C" int cupf_abi_version(void) { return CUPF_ABI_VERSION; }
@@ -75,7 +70,8 @@ struct cupf_apt_handle {
   int device = 0;
   cupf_precision prec = CUPF_PREC_FP32;
   Grid g;
-  uint2* buf[2] = {nullptr, nullptr};
+  int pair_bytes = 8;
+  void* buf[2] = {nullptr, nullptr};
   CUtensorMap tmap[2];
   int cur = 0;  // buffer holding the current state
   int64_t steps_done = 0;
@@ -90,6 +86,8 @@ struct cupf_apt_handle {
   float* phi_m = nullptr;
   int* alpha_m = nullptr;
   int* err = nullptr;
+  int* work = nullptr;  // persistent-launch work counter [next, done]
+  int grid_cap = 0;     // resident CTAs of the step kernel (occupancy x SMs)
   // read-back scratch (reference layout, num_pf * length), allocated on first use
   float* xfer_ph = nullptr;
   int* xfer_id = nullptr;
@@ -101,6 +99,7 @@ struct cupf_apt_handle {
   // reductions
   unsigned long long* counts = nullptr;
   long long* first = nullptr;
+  double* qoi_part = nullptr;
   int counts_cap = 0;
   // launch shape
   int zc = 64;
@@ -121,30 +120,62 @@ static cupf_status upload(float** dst, const float* src, size_t n, cudaStream_t 
   return CUPF_OK;
 }
 
+// Call f(S{}) with the storage format S of the handle.
+template <class F>
+static cupf_status with_storage(cupf_precision prec, F&& f) {
+  switch (prec) {
+    case CUPF_PREC_FP32: return f(PairF32{});
+    case CUPF_PREC_BF16: return f(PairBF16{});
+    case CUPF_PREC_FP16: return f(PairFP16{});
+  }
+  return fail(CUPF_ERR_UNSUPPORTED, "precision %d", (int)prec);
+}
+
+template <class S>
+static typename S::T* B(void* p) {
+  return static_cast<typename S::T*>(p);
+}
+
+// launch kernel<S> for the handle's storage format; buffers cast with B<S>(...)
+#define LAUNCH_S(h, kernel, grid, block, ...)                                   \
+  do {                                                                          \
+    cupf_status st_ = with_storage((h)->prec, [&](auto tag) -> cupf_status {    \
+      using S = decltype(tag);                                                  \
+      kernel<S><<<(grid), (block), 0, (h)->stream>>>(__VA_ARGS__);              \
+      return CUPF_OK;                                                           \
+    });                                                                         \
+    if (st_) return st_;                                                        \
+  } while (0)
+
 static cupf_status make_tmap(cupf_apt_handle* h, int b) {
   EncodeTiledFn enc = get_encode();
   if (!enc) return fail(CUPF_ERR_CUDA, "cuTensorMapEncodeTiled entry point not available");
   const Grid& g = h->g;
-  cuuint64_t dims[4] = {(cuuint64_t)g.fnx, (cuuint64_t)g.fny, (cuuint64_t)g.fnz,
-                        (cuuint64_t)g.np};
-  cuuint64_t strides[3] = {(cuuint64_t)g.xp * 8, (cuuint64_t)g.xp * g.fny * 8,
-                           (cuuint64_t)g.ss * 8};
-  cuuint32_t box[4] = {(cuuint32_t)BW, (cuuint32_t)BH, 1u, (cuuint32_t)g.np};
-  cuuint32_t es[4] = {1, 1, 1, 1};
-  CUresult r = enc(&h->tmap[b], CU_TENSOR_MAP_DATA_TYPE_UINT64, 4, h->buf[b], dims, strides, box,
-                   es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return fail(CUPF_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
-  return CUPF_OK;
+  return with_storage(h->prec, [&](auto tag) -> cupf_status {
+    using S = decltype(tag);
+    const cuuint64_t e = S::kBytes;
+    cuuint64_t dims[4] = {(cuuint64_t)g.fnx, (cuuint64_t)g.fny, (cuuint64_t)g.fnz,
+                          (cuuint64_t)g.np};
+    cuuint64_t strides[3] = {(cuuint64_t)g.xp * e, (cuuint64_t)g.xp * g.fny * e,
+                             (cuuint64_t)g.ss * e};
+    cuuint32_t box[4] = {(cuuint32_t)S::kBW, (cuuint32_t)BH, 1u, (cuuint32_t)g.np};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    CUresult r = enc(&h->tmap[b], S::kTmaType, 4, h->buf[b], dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+      return fail(CUPF_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return CUPF_OK;
+  });
 }
 
 static void free_handle(cupf_apt_handle* h) {
   if (!h) return;
   cudaSetDevice(h->device);
   void* ptrs[] = {h->buf[0], h->buf[1], h->x, h->y, h->z, h->sint, h->cost, h->X_mac, h->Y_mac,
-                  h->Z_mac, h->t_mac, h->psi_mac, h->T_3D, h->phi_m, h->alpha_m, h->err,
+                  h->Z_mac, h->t_mac, h->psi_mac, h->T_3D, h->phi_m, h->alpha_m, h->err, h->work,
                   h->xfer_ph, h->xfer_id, h->layer_sums, h->alpha_full, h->loss_area,
-                  h->counts, h->first};
+                  h->counts, h->first, h->qoi_part};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -154,31 +185,41 @@ static void free_handle(cupf_apt_handle* h) {
 }
 
 // ------------------------------------------------------------------ step launch
-template <int NP>
+template <int NP, class S>
 static cupf_status launch_step_np(cupf_apt_handle* h, const StepArgs& a, const CUtensorMap& m) {
   static bool configured[64] = {};
-  const int bytes = StepSmem<NP>::kBytes;
+  static int resident[64] = {};
+  const int bytes = StepSmem<NP, S>::kBytes;
   if (!configured[h->device & 63]) {
-    CK(cudaFuncSetAttribute(apt_step_kernel<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CK(cudaFuncSetAttribute(apt_step_kernel<NP, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             bytes));
+    int per_sm = 0, nsm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, apt_step_kernel<NP, S>, NTHREADS,
+                                                     bytes));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+    resident[h->device & 63] = std::max(1, per_sm) * nsm;
     configured[h->device & 63] = true;
   }
-  const int nblk = h->ntx * h->nty * h->nzc;
-  apt_step_kernel<NP><<<nblk, NTHREADS, bytes, h->stream>>>(m, a);
+  const int nitems = h->ntx * h->nty * h->nzc;
+  const int nblk = std::min(nitems, h->grid_cap > 0 ? h->grid_cap : resident[h->device & 63]);
+  apt_step_kernel<NP, S><<<nblk, NTHREADS, bytes, h->stream>>>(m, a);
   CK(cudaGetLastError());
   return CUPF_OK;
 }
 
 static cupf_status launch_step(cupf_apt_handle* h, const StepArgs& a, const CUtensorMap& m) {
-  switch (h->g.np) {
+  return with_storage(h->prec, [&](auto tag) -> cupf_status {
+    using S = decltype(tag);
+    switch (h->g.np) {
 #define CASE(N) \
   case N:       \
-    return launch_step_np<N>(h, a, m);
-    CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8)
+    return launch_step_np<N, S>(h, a, m);
+      CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8)
 #undef CASE
-    default:
-      return fail(CUPF_ERR_UNSUPPORTED, "num_pf=%d not built (1..8)", h->g.np);
-  }
+      default:
+        return fail(CUPF_ERR_UNSUPPORTED, "num_pf=%d not built (1..8)", h->g.np);
+    }
+  });
 }
 
 static StepArgs step_args(cupf_apt_handle* h, float t, int use_iuc) {
@@ -211,6 +252,7 @@ static StepArgs step_args(cupf_apt_handle* h, float t, int use_iuc) {
   a.hi = p.hi;
   a.lamd = p.lamd;
   a.dt = p.dt;
+  a.tau0 = p.tau0;
   a.lyd = p.lyd;
   a.lzd = p.lzd;
   a.r0 = p.r0;
@@ -232,6 +274,7 @@ static StepArgs step_args(cupf_apt_handle* h, float t, int use_iuc) {
   a.Z_mac = h->Z_mac;
   a.psi_mac = h->psi_mac;
   a.err = h->err;
+  a.work = h->work;
   return a;
 }
 
@@ -274,8 +317,10 @@ extern "C" cupf_status cupf_apt_create(const cupf_apt_params* p, const cupf_apt_
   if (p->haloWidth != 1) return fail(CUPF_ERR_INVALID, "haloWidth must be 1");
   if (p->thermalType < 0 || p->thermalType > 4)
     return fail(CUPF_ERR_INVALID, "thermalType %d not in 0..4", p->thermalType);
-  if (precision != CUPF_PREC_FP32)
+  if (precision != CUPF_PREC_FP32 && precision != CUPF_PREC_BF16 && precision != CUPF_PREC_FP16)
     return fail(CUPF_ERR_UNSUPPORTED, "precision %d not built", (int)precision);
+  if (precision != CUPF_PREC_FP32 && p->num_theta > 32767)
+    return fail(CUPF_ERR_UNSUPPORTED, "16-bit storage keeps grain ids in int16 (num_theta <= 32767)");
   if (!in->x || !in->y || !in->z || !in->sint || !in->cost)
     return fail(CUPF_ERR_INVALID, "x, y, z, sint and cost are required");
   if (p->thermalType == 4 && (!in->X_mac || !in->Y_mac || !in->Z_mac || !in->psi_mac))
@@ -288,7 +333,9 @@ extern "C" cupf_status cupf_apt_create(const cupf_apt_params* p, const cupf_apt_
   h->g.fnx = p->fnx;
   h->g.fny = p->fny;
   h->g.fnz = p->fnz;
-  h->g.xp = (p->fnx + 1) & ~1;
+  h->pair_bytes = precision == CUPF_PREC_FP32 ? 8 : 4;
+  const int palign = precision == CUPF_PREC_FP32 ? PairF32::kPitchAlign : PairBF16::kPitchAlign;
+  h->g.xp = (p->fnx + palign - 1) / palign * palign;
   h->g.np = p->num_pf;
   h->g.ss = (long long)h->g.xp * p->fny * p->fnz;
   cupf_status st = CUPF_OK;
@@ -309,7 +356,7 @@ extern "C" cupf_status cupf_apt_create(const cupf_apt_params* p, const cupf_apt_
   TRY(cuda(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream"));
   TRY(cuda(cudaEventCreate(&h->ev0), "event"));
   TRY(cuda(cudaEventCreate(&h->ev1), "event"));
-  const size_t bbytes = (size_t)h->g.ss * h->g.np * sizeof(uint2);
+  const size_t bbytes = (size_t)h->g.ss * h->g.np * h->pair_bytes;
   for (int b = 0; b < 2; ++b) {
     TRY(cuda(cudaMalloc((void**)&h->buf[b], bbytes), "slot buffer"));
     TRY(cuda(cudaMemsetAsync(h->buf[b], 0xFF, bbytes, h->stream), "memset"));
@@ -336,6 +383,8 @@ extern "C" cupf_status cupf_apt_create(const cupf_apt_params* p, const cupf_apt_
   TRY(cuda(cudaMemsetAsync(h->alpha_m, 0, L * sizeof(int), h->stream), "memset"));
   TRY(cuda(cudaMalloc((void**)&h->err, sizeof(int)), "err"));
   TRY(cuda(cudaMemsetAsync(h->err, 0, sizeof(int), h->stream), "memset"));
+  TRY(cuda(cudaMalloc((void**)&h->work, 2 * sizeof(int)), "work"));
+  TRY(cuda(cudaMemsetAsync(h->work, 0, 2 * sizeof(int), h->stream), "memset"));
   TRY(cuda(cudaMalloc((void**)&h->layer_sums, p->fnz * sizeof(double)), "layer sums"));
   for (int b = 0; b < 2; ++b) TRY(make_tmap(h, b));
   const char* zc_env = getenv("CUPF_ZC");
@@ -356,15 +405,26 @@ extern "C" cupf_status cupf_apt_destroy(cupf_apt_handle* h) {
 
 extern "C" void* cupf_apt_stream(cupf_apt_handle* h) { return h ? (void*)h->stream : nullptr; }
 
+extern "C" cupf_status cupf_apt_set_tuning(cupf_apt_handle* h, int32_t z_chunk) {
+  if (!h) return fail(CUPF_ERR_INVALID, "null handle");
+  if (z_chunk < 1) return fail(CUPF_ERR_INVALID, "z_chunk must be >= 1");
+  set_zc(h, z_chunk);
+  return CUPF_OK;
+}
+
 extern "C" cupf_status cupf_apt_init_from_argmax(cupf_apt_handle* h, const float* phi,
                                                  const int32_t* alpha) {
   if (!h || !phi || !alpha) return fail(CUPF_ERR_INVALID, "null argument");
   CK(cudaSetDevice(h->device));
   const size_t L = (size_t)h->g.length();
+  const int id_max = h->prec == CUPF_PREC_FP32 ? 0x7FFFFFFF : 32767;
+  for (size_t i = 0; i < L; ++i)
+    if ((double)phi[i] > LS && (alpha[i] < -1 || alpha[i] > id_max))
+      return fail(CUPF_ERR_INVALID, "grain id %d at %zu outside [-1, %d]", alpha[i], i, id_max);
   CK(cudaMemcpyAsync(h->phi_m, phi, L * sizeof(float), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->alpha_m, alpha, L * sizeof(int), cudaMemcpyHostToDevice, h->stream));
-  init_kernel<<<grid_for(L), 256, 0, h->stream>>>(h->buf[0], h->buf[1], h->phi_m, h->alpha_m,
-                                                   h->g);
+  LAUNCH_S(h, init_kernel, grid_for(L), 256, B<S>(h->buf[0]), B<S>(h->buf[1]), h->phi_m,
+           h->alpha_m, h->g);
   CK(cudaGetLastError());
   h->cur = 0;
   h->steps_done = 0;
@@ -387,14 +447,16 @@ extern "C" cupf_status cupf_apt_set_slots(cupf_apt_handle* h, const float* ph, c
   if (!h || !ph || !ids) return fail(CUPF_ERR_INVALID, "null argument");
   CK(cudaSetDevice(h->device));
   const size_t n = (size_t)h->g.length() * h->g.np;
+  const int id_max = h->prec == CUPF_PREC_FP32 ? 0x7FFFFFFF : 32767;
   for (size_t i = 0; i < n; ++i)
-    if (ids[i] < -1) return fail(CUPF_ERR_INVALID, "grain id %d at %zu (ids must be >= -1)", ids[i], i);
+    if (ids[i] < -1 || ids[i] > id_max)
+      return fail(CUPF_ERR_INVALID, "grain id %d at %zu outside [-1, %d]", ids[i], i, id_max);
   cupf_status st = ensure_xfer(h);
   if (st) return st;
   CK(cudaMemcpyAsync(h->xfer_ph, ph, n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->xfer_id, ids, n * sizeof(int), cudaMemcpyHostToDevice, h->stream));
-  import_kernel<<<grid_for(n), 256, 0, h->stream>>>(h->buf[0], h->xfer_ph, h->xfer_id, h->g);
-  import_kernel<<<grid_for(n), 256, 0, h->stream>>>(h->buf[1], h->xfer_ph, h->xfer_id, h->g);
+  LAUNCH_S(h, import_kernel, grid_for(n), 256, B<S>(h->buf[0]), h->xfer_ph, h->xfer_id, h->g);
+  LAUNCH_S(h, import_kernel, grid_for(n), 256, B<S>(h->buf[1]), h->xfer_ph, h->xfer_id, h->g);
   CK(cudaGetLastError());
   h->cur = 0;
   h->steps_done = steps_done;
@@ -406,7 +468,8 @@ extern "C" cupf_status cupf_apt_set_slots(cupf_apt_handle* h, const float* ph, c
 static cupf_status fill_halo(cupf_apt_handle* h, int b) {
   const Grid& g = h->g;
   const long long n = 2ll * g.fnx * g.fny + 2ll * g.fnx * (g.fnz - 2) + 2ll * (g.fny - 2) * (g.fnz - 2);
-  fill_halo_kernel<<<grid_for(n), 256, 0, h->stream>>>(h->buf[b], g, h->p.bcX, h->p.bcY, h->p.bcZ);
+  LAUNCH_S(h, fill_halo_kernel, grid_for(n), 256, B<S>(h->buf[b]), g, h->p.bcX, h->p.bcY,
+           h->p.bcZ);
   CK(cudaGetLastError());
   return CUPF_OK;
 }
@@ -419,7 +482,8 @@ extern "C" cupf_status cupf_apt_get_slots(cupf_apt_handle* h, float* ph, int32_t
   if (st) return st;
   if ((st = fill_halo(h, h->cur))) return st;
   const size_t n = (size_t)h->g.length() * h->g.np;
-  export_kernel<<<grid_for(n), 256, 0, h->stream>>>(h->buf[h->cur], h->xfer_ph, h->xfer_id, h->g);
+  LAUNCH_S(h, export_kernel, grid_for(n), 256, B<S>(h->buf[h->cur]), h->xfer_ph, h->xfer_id,
+           h->g);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(ph, h->xfer_ph, n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaMemcpyAsync(ids, h->xfer_id, n * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -465,7 +529,7 @@ extern "C" cupf_status cupf_apt_collect(cupf_apt_handle* h, int32_t clear, float
   }
   cupf_status st = fill_halo(h, h->cur);
   if (st) return st;
-  collect_kernel<<<grid_for(L), 256, 0, h->stream>>>(h->buf[h->cur], h->phi_m, h->alpha_m, h->g);
+  LAUNCH_S(h, collect_kernel, grid_for(L), 256, B<S>(h->buf[h->cur]), h->phi_m, h->alpha_m, h->g);
   CK(cudaGetLastError());
   if (phi_out)
     CK(cudaMemcpyAsync(phi_out, h->phi_m, L * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
@@ -502,6 +566,32 @@ extern "C" cupf_status cupf_apt_grain_volumes(cupf_apt_handle* h, int32_t num_gr
   return CUPF_OK;
 }
 
+extern "C" cupf_status cupf_apt_qoi_sums(cupf_apt_handle* h, double* out) {
+  if (!h || !out) return fail(CUPF_ERR_INVALID, "null argument");
+  if (!h->initialised) return fail(CUPF_ERR_STATE, "state not initialised");
+  CK(cudaSetDevice(h->device));
+  const int nb = 148 * 4;
+  if (!h->qoi_part) CK(cudaMalloc((void**)&h->qoi_part, 2 * nb * sizeof(double)));
+  cupf_status st = fill_halo(h, h->cur);
+  if (st) return st;
+  LAUNCH_S(h, qoi_sums_kernel, nb, 256, B<S>(h->buf[h->cur]), h->g, h->qoi_part);
+  CK(cudaGetLastError());
+  std::vector<double> part(2 * nb);
+  CK(cudaMemcpyAsync(part.data(), h->qoi_part, part.size() * sizeof(double),
+                     cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  double v = 0.0, a = 0.0;
+  for (int b = 0; b < nb; ++b) {
+    v += part[2 * b];
+    a += part[2 * b + 1];
+  }
+  const double base = (double)(h->p.fnx - 2) * (h->p.fny - 2);
+  out[0] = v;
+  out[1] = a;
+  out[2] = v / base;
+  return check_err_word(h);
+}
+
 extern "C" cupf_status cupf_apt_move_domain(cupf_apt_handle* h, int32_t* tip_front,
                                             int32_t tip_thres, int32_t* move_count,
                                             int32_t* moved) {
@@ -520,7 +610,7 @@ extern "C" cupf_status cupf_apt_move_domain(cupf_apt_handle* h, int32_t* tip_fro
   }
   cupf_status st = fill_halo(h, h->cur);
   if (st) return st;
-  layer_sum_kernel<<<p.fnz, 256, 0, h->stream>>>(h->buf[h->cur], h->layer_sums, g);
+  LAUNCH_S(h, layer_sum_kernel, p.fnz, 256, B<S>(h->buf[h->cur]), h->layer_sums, g);
   CK(cudaGetLastError());
   std::vector<double> sums(p.fnz);
   CK(cudaMemcpyAsync(sums.data(), h->layer_sums, p.fnz * sizeof(double), cudaMemcpyDeviceToHost,
@@ -546,13 +636,13 @@ extern "C" cupf_status cupf_apt_move_domain(cupf_apt_handle* h, int32_t* tip_fro
       h->fnz_f = nf;
     }
     const size_t L = (size_t)g.length();
-    collect_kernel<<<grid_for(L), 256, 0, h->stream>>>(h->buf[h->cur], h->phi_m, h->alpha_m, g);
+    LAUNCH_S(h, collect_kernel, grid_for(L), 256, B<S>(h->buf[h->cur]), h->phi_m, h->alpha_m, g);
     archive_kernel<<<grid_for(plane), 256, 0, h->stream>>>(h->alpha_m, h->alpha_full, h->loss_area,
                                                            p.fnx, p.fny, *move_count, p.num_theta);
     const long long ni = (long long)(p.fnx - 2) * (p.fny - 2) * (p.fnz - 2) * p.num_pf;
-    shift_kernel<<<grid_for(ni), 256, 0, h->stream>>>(h->buf[h->cur], h->buf[h->cur ^ 1], g);
-    copy_interior_kernel<<<grid_for(ni), 256, 0, h->stream>>>(h->buf[h->cur ^ 1], h->buf[h->cur],
-                                                              g);
+    LAUNCH_S(h, shift_kernel, grid_for(ni), 256, B<S>(h->buf[h->cur]), B<S>(h->buf[h->cur ^ 1]), g);
+    LAUNCH_S(h, copy_interior_kernel, grid_for(ni), 256, B<S>(h->buf[h->cur ^ 1]),
+             B<S>(h->buf[h->cur]), g);
     CK(cudaGetLastError());
     // z shift (APTmove_frame :365-369 then APTcopy_frame :401-402)
     std::vector<float>& z = h->z_host;

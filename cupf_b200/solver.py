@@ -105,6 +105,12 @@ class APTSolver:
                                                 c.ctypes.data_as(C.POINTER(C.c_int64))))
         return c
 
+    def qoi_sums(self):
+        """(solid volume, interface area, mean interface height) in FP64, cell units."""
+        out = (C.c_double * 3)()
+        abi.check(self.L.cupf_apt_qoi_sums(self.h, out))
+        return tuple(out)
+
     def move_domain(self, tip_front, tip_thres, move_count):
         tf = C.c_int32(tip_front)
         mc = C.c_int32(move_count)
@@ -132,6 +138,9 @@ class APTSolver:
         ms = C.c_float()
         abi.check(self.L.cupf_apt_time_steps(self.h, int(nsteps), C.byref(ms)))
         return ms.value
+
+    def set_tuning(self, z_chunk):
+        abi.check(self.L.cupf_apt_set_tuning(self.h, int(z_chunk)))
 
     @property
     def stream(self):

@@ -172,6 +172,16 @@ cupf_status cupf_apt_collect(cupf_apt_handle* h, int32_t clear, float* phi_out,
 cupf_status cupf_apt_grain_volumes(cupf_apt_handle* h, int32_t num_grains,
                                    int64_t* counts);
 
+/* FP64 interface quantities of the current state, over interior cells, from
+ * the per-cell maximum of phi over the slots (m):
+ *   out[0] = sum (1+m)/2            solid volume in cells
+ *   out[1] = sum |grad m|/2         interface area in cell faces (central differences)
+ *   out[2] = out[0] / (interior cells per layer)   mean interface height in cells
+ * Reduced in double in a fixed order (deterministic).  Supplies the volume and
+ * interface measures the split-precision error is judged on; the reference has
+ * no counterpart (its QoIs are integer voxel counts, QOI.cpp:38-231). */
+cupf_status cupf_apt_qoi_sums(cupf_apt_handle* h, double* out);
+
 /* Moving-domain check and shift (line configuration).  Computes the per-layer
  * mean of phi over all slots and cells, advances *tip_front while the mean is
  * above LS, and while *tip_front >= tip_thres shifts the window down one layer:
@@ -206,6 +216,59 @@ cupf_status cupf_apt_time_steps(cupf_apt_handle* h, int32_t nsteps, float* ms);
 /* Raw stream of the handle (a cudaStream_t), for callers that order their own
  * work after the solver's. */
 void* cupf_apt_stream(cupf_apt_handle* h);
+
+/* Launch shape of the step kernel: z_chunk = interior planes per CTA work item
+ * (the column tile is fixed at 32 x 8).  No reference counterpart (the
+ * reference marches every column over the whole height, APTPhaseField.cu:190). */
+cupf_status cupf_apt_set_tuning(cupf_apt_handle* h, int32_t z_chunk);
+
+/* ---------------------------------------------------------------- serving
+ * Continuous batching of independent simulations on one GPU.  No reference
+ * counterpart: the reference runs one simulation per process (main.cpp:15-77).
+ * Requests of any grid size queue FIFO; cupf_server_pump retires finished
+ * simulations (argmax map, per-grain volumes and FP64 interface sums copied to
+ * host memory), admits queued ones while a slot and HBM within the budget are
+ * free, and advances every resident simulation steps_per_round steps in one
+ * persistent batched kernel per step, replayed from a captured CUDA graph.
+ * A request's results are identical whether it runs alone or batched. */
+typedef struct cupf_server cupf_server;
+
+typedef struct cupf_server_config {
+  int32_t device;
+  int32_t precision;        /* cupf_precision, shared by every request */
+  int32_t num_pf;           /* NUM_PF, shared by every request */
+  int32_t max_active;       /* resident simulations at most */
+  int32_t steps_per_round;  /* steps per graph replay (one pump) */
+  int32_t autotune;         /* 1: pick the z chunk of each grid shape by timing */
+  int64_t hbm_budget_bytes; /* device memory for requests; 0 = free memory - 2 GiB */
+} cupf_server_config;
+
+cupf_status cupf_server_create(const cupf_server_config* cfg, cupf_server** out);
+cupf_status cupf_server_destroy(cupf_server* s);
+
+/* Queue a simulation: parameters and inputs as for cupf_apt_create, initial
+ * argmax fields as for cupf_apt_init_from_argmax (all copied), nsteps explicit
+ * steps (line / cylinder thermal types).  *request_id identifies it. */
+cupf_status cupf_server_submit(cupf_server* s, const cupf_apt_params* p,
+                               const cupf_apt_inputs* in, const float* phi,
+                               const int32_t* alpha, int64_t nsteps, int64_t* request_id);
+
+/* One scheduling round (see above); blocks until the round's steps are done.
+ * Any output pointer may be NULL. */
+cupf_status cupf_server_pump(cupf_server* s, int32_t* n_running, int32_t* n_pending,
+                             int32_t* n_done);
+
+/* State of a request (0 pending, 1 running, 2 done, 3 failed) and, when done,
+ * its results: argmax grain map (length ints, as cupf_apt_collect with clear),
+ * voxel counts per grain id 0..num_grains (as cupf_apt_grain_volumes), the three
+ * FP64 sums of cupf_apt_qoi_sums, and the host clock (seconds) at submit,
+ * admission and completion.  Output pointers may be NULL. */
+cupf_status cupf_server_result(cupf_server* s, int64_t id, int32_t* status, int32_t* alpha_out,
+                               int64_t* volumes_out, int32_t num_grains, double* qoi_out,
+                               double* times_out);
+
+/* Forget a finished (or still queued) request and its host results. */
+cupf_status cupf_server_release(cupf_server* s, int64_t id);
 
 #ifdef __cplusplus
 }
