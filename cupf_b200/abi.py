@@ -95,6 +95,9 @@ def lib():
             "cupf_apt_sync": [vp, C.c_int32],
             "cupf_apt_time_steps": [vp, C.c_int32, FP],
             "cupf_apt_set_tuning": [vp, C.c_int32],
+            "cupf_apt_nucl_init": [vp],
+            "cupf_apt_nucleate": [vp, C.c_int32, C.POINTER(C.c_int32)],
+            "cupf_apt_nucl_reset": [vp],
             "cupf_server_create": [C.POINTER(cupf_server_config), C.POINTER(vp)],
             "cupf_server_destroy": [vp],
             "cupf_server_submit": [vp, C.POINTER(cupf_apt_params), C.POINTER(cupf_apt_inputs), FP,

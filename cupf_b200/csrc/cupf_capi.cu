@@ -19,6 +19,7 @@
 
 #include "../../include/cupf.h"
 #include "apt_aux.cuh"
+#include "apt_nucl.cuh"
 #include "capi_internal.h"
 #include "apt_step.cuh"
 
@@ -81,6 +82,7 @@ struct cupf_apt_handle {
   float *x = nullptr, *y = nullptr, *z = nullptr, *sint = nullptr, *cost = nullptr;
   float *X_mac = nullptr, *Y_mac = nullptr, *Z_mac = nullptr, *t_mac = nullptr;
   float *psi_mac = nullptr, *T_3D = nullptr;
+  bool has_T3D = false;
   std::vector<float> z_host;
   // argmax fields (reference layout, length)
   float* phi_m = nullptr;
@@ -100,6 +102,11 @@ struct cupf_apt_handle {
   unsigned long long* counts = nullptr;
   long long* first = nullptr;
   double* qoi_part = nullptr;
+  // nucleation
+  int* nucl_status = nullptr;
+  int* nucl_count = nullptr;
+  float* nucl_sphere = nullptr;
+  int cnx = 0, cny = 0, cnz = 0, pts = 0;
   int counts_cap = 0;
   // launch shape
   int zc = 64;
@@ -175,7 +182,8 @@ static void free_handle(cupf_apt_handle* h) {
   void* ptrs[] = {h->buf[0], h->buf[1], h->x, h->y, h->z, h->sint, h->cost, h->X_mac, h->Y_mac,
                   h->Z_mac, h->t_mac, h->psi_mac, h->T_3D, h->phi_m, h->alpha_m, h->err, h->work,
                   h->xfer_ph, h->xfer_id, h->layer_sums, h->alpha_full, h->loss_area,
-                  h->counts, h->first, h->qoi_part};
+                  h->counts, h->first, h->qoi_part, h->nucl_status, h->nucl_count,
+                  h->nucl_sphere};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -376,6 +384,7 @@ extern "C" cupf_status cupf_apt_create(const cupf_apt_params* p, const cupf_apt_
   TRY(upload(&h->t_mac, in->t_mac, in->t_mac ? mNt : 2, h->stream));
   TRY(upload(&h->psi_mac, in->psi_mac, in->psi_mac ? mNx * mNy * mNz : 8, h->stream));
   TRY(upload(&h->T_3D, in->T_3D, in->T_3D ? mNx * mNy * mNz * mNt : 16, h->stream));
+  h->has_T3D = in->T_3D != nullptr;
   const size_t L = (size_t)h->g.length();
   TRY(cuda(cudaMalloc((void**)&h->phi_m, L * sizeof(float)), "phi"));
   TRY(cuda(cudaMalloc((void**)&h->alpha_m, L * sizeof(int)), "alpha"));
@@ -590,6 +599,114 @@ extern "C" cupf_status cupf_apt_qoi_sums(cupf_apt_handle* h, double* out) {
   out[1] = a;
   out[2] = v / base;
   return check_err_word(h);
+}
+
+static NuclArgs nucl_args(cupf_apt_handle* h, int use_iuc) {
+  const cupf_apt_params& p = h->p;
+  NuclArgs a;
+  memset(&a, 0, sizeof(a));
+  a.fnx = p.fnx;
+  a.fny = p.fny;
+  a.fnz = p.fnz;
+  a.xp = h->g.xp;
+  a.slot_stride = h->g.ss;
+  a.np = h->g.np;
+  a.cnx = h->cnx;
+  a.cny = h->cny;
+  a.cnz = h->cnz;
+  a.pts = h->pts;
+  a.num_theta = p.num_theta;
+  a.id_space = h->prec == CUPF_PREC_FP32 ? (1 << 30) : (32767 - p.num_theta);
+  a.use_iuc = use_iuc;
+  a.uc0 = p.underCoolingRate0;
+  a.nmax0 = p.nuc_Nmax0;
+  a.nmax = p.nuc_Nmax;
+  a.mean = p.undcool_mean;
+  a.std = p.undcool_std;
+  a.rad = p.nuc_rad;
+  a.dt2 = 2.0f * p.dt * p.tau0;
+  a.t = (float)h->steps_done * p.dt * p.tau0;
+  a.seed = (uint32_t)p.seed;
+  a.step = (uint32_t)h->steps_done;
+  a.T_3D = h->has_T3D ? h->T_3D : nullptr;
+  a.X_mac = h->X_mac;
+  a.Y_mac = h->Y_mac;
+  a.Z_mac = h->Z_mac;
+  a.t_mac = h->t_mac;
+  a.x = h->x;
+  a.y = h->y;
+  a.z = h->z;
+  a.Nx = p.Nx;
+  a.Ny = p.Ny;
+  a.Nz = p.Nz;
+  a.Nt = p.Nt;
+  a.sphere = h->nucl_sphere;
+  a.status = h->nucl_status;
+  a.count = h->nucl_count;
+  return a;
+}
+
+extern "C" cupf_status cupf_apt_nucl_init(cupf_apt_handle* h) {
+  if (!h) return fail(CUPF_ERR_INVALID, "null handle");
+  if (!h->initialised) return fail(CUPF_ERR_STATE, "state not initialised");
+  const cupf_apt_params& p = h->p;
+  if (p.pts_cell < 0 || p.dx <= 0 || p.sqrt2 <= 0)
+    return fail(CUPF_ERR_INVALID, "nucleation needs pts_cell >= 0, dx and sqrt2");
+  if (h->prec != CUPF_PREC_FP32 && p.num_theta >= 32767)
+    return fail(CUPF_ERR_UNSUPPORTED, "no id space left for nuclei in int16 storage");
+  CK(cudaSetDevice(h->device));
+  const int w = 2 * p.pts_cell + 1;
+  h->pts = p.pts_cell;
+  h->cnx = (p.fnx - 1 - 2) / w;
+  h->cny = (p.fny - 1 - 2) / w;
+  h->cnz = (p.fnz - 1 - 2) / w;
+  const long long nc = (long long)h->cnx * h->cny * h->cnz;
+  if (nc < 1) return fail(CUPF_ERR_INVALID, "grid smaller than one nucleation cell");
+  if (!h->nucl_status) {
+    CK(cudaMalloc((void**)&h->nucl_status, nc * sizeof(int)));
+    CK(cudaMalloc((void**)&h->nucl_count, sizeof(int)));
+    CK(cudaMalloc((void**)&h->nucl_sphere, (size_t)w * w * w * sizeof(float)));
+  }
+  // nucleus profile (add_nucl :515-528): tanh(dx*((1+pts)/2 - |offset|) / sqrt2)
+  std::vector<float> sph((size_t)w * w * w);
+  const float pf = (float)p.pts_cell;
+  for (int k = -p.pts_cell; k <= p.pts_cell; ++k)
+    for (int j = -p.pts_cell; j <= p.pts_cell; ++j)
+      for (int i = -p.pts_cell; i <= p.pts_cell; ++i) {
+        const float d = p.dx * ((1.0f + pf) / 2.0f - sqrtf((float)(i * i + j * j + k * k)));
+        sph[((k + p.pts_cell) * w + (j + p.pts_cell)) * w + (i + p.pts_cell)] = tanhf(d / p.sqrt2);
+      }
+  CK(cudaMemcpyAsync(h->nucl_sphere, sph.data(), sph.size() * sizeof(float),
+                     cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemsetAsync(h->nucl_count, 0, sizeof(int), h->stream));
+  NuclArgs a = nucl_args(h, 0);
+  LAUNCH_S(h, nucl_status_init_kernel, grid_for(nc), 256, B<S>(h->buf[h->cur]), a);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->stream));
+  return CUPF_OK;
+}
+
+extern "C" cupf_status cupf_apt_nucl_reset(cupf_apt_handle* h) {
+  if (!h || !h->nucl_status) return fail(CUPF_ERR_STATE, "nucleation not initialised");
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemsetAsync(h->nucl_status, 0,
+                     (size_t)h->cnx * h->cny * h->cnz * sizeof(int), h->stream));
+  return CUPF_OK;
+}
+
+extern "C" cupf_status cupf_apt_nucleate(cupf_apt_handle* h, int32_t use_initial_undercooling,
+                                         int32_t* total) {
+  if (!h || !h->nucl_status) return fail(CUPF_ERR_STATE, "nucleation not initialised");
+  CK(cudaSetDevice(h->device));
+  const long long nc = (long long)h->cnx * h->cny * h->cnz;
+  NuclArgs a = nucl_args(h, use_initial_undercooling);
+  LAUNCH_S(h, nucleate_kernel, grid_for(nc), 256, B<S>(h->buf[h->cur]), a);
+  CK(cudaGetLastError());
+  if (total) {
+    CK(cudaMemcpyAsync(total, h->nucl_count, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  return CUPF_OK;
 }
 
 extern "C" cupf_status cupf_apt_move_domain(cupf_apt_handle* h, int32_t* tip_front,

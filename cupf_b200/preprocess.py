@@ -1,0 +1,84 @@
+"""Writers of the reference's driver inputs: the `forcing/case<seed>/` folder and
+the `line.py`-style input file read by `phase_field`.
+
+File names, formats and meanings follow the reference's pre-processing
+(3DgrainMPI/grains3D.py:337-378: one value per line, "%1.4e" for reals, "%d" for
+integers) and its line input file (3DgrainMPI/line.py); the thermal model is the
+line profile psi = z0 - z on a coarse macro grid spanning [-BC, L+BC]
+(grains3D.py:258-260, TemperatureProfile3DAnalytic.py).
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+
+from .cases import LINE_CONSTANTS, grain_angles, voronoi_substrate
+
+INPUT_KEYS = ["Tmelt", "Dh", "L_cp", "GT", "beta0", "mu_k", "delta", "kin_delta",
+              "undcool_mean", "undcool_std", "nuc_Nmax", "nuc_rad", "eps", "dx", "W0", "cfl"]
+
+
+def write_input_file(path, Lx, nts=2, asp_ratio_yx=1.0, asp_ratio_zx=2.0, moving_ratio=1.0,
+                     macro=(13, 13, 23, 11), num_pf=8, extra=None):
+    """A line.py-style parameter file (`key = value` per line)."""
+    vals = dict(LINE_CONSTANTS)
+    if extra:
+        vals.update(extra)
+    lines = ["# parameters of a line (frozen-gradient) run"]
+    for k in INPUT_KEYS:
+        lines.append("%s = %r" % (k, vals[k]))
+    lines += ["underCoolingRate0 = %r" % vals["underCoolingRate0"], "nuc_Nmax0 = 0.01",
+              "nx = %d" % macro[0], "ny = %d" % macro[1], "nz = %d" % macro[2],
+              "nt = %d" % macro[3], "haloWidth = 1", "xmin = 0", "ymin = 0", "zmin = 0",
+              "eta = 0.0", "noi_period = 200", "ictype = 0", "asp_ratio_yx = %r" % asp_ratio_yx,
+              "asp_ratio_zx = %r" % asp_ratio_zx, "moving_ratio = %r" % moving_ratio,
+              "nts = %d" % nts, "Lx = %r" % Lx, "preMt = 0", "NUM_PF = %d" % num_pf]
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+def write_line_forcing(folder, Lx, Ly, Lz, num_grains, seed, G, R, z0, top, t_end,
+                       periodic=True, macro=(13, 13, 23, 11), dxd=0.08):
+    """The forcing folder of a line run: macro grid, psi = z0 - z, substrate ids
+    (alpha.txt, (nx+1)x(ny+1) values), orientations, scalars."""
+    os.makedirs(folder, exist_ok=True)
+    nxm, nym, nzm, ntm = macro
+    BC = Lx / (nxm - 3)
+    x = np.linspace(0 - BC, Lx + BC, nxm)
+    y = np.linspace(0 - BC, Ly + BC, nym)
+    z = np.linspace(0 - BC, Lz + BC, nzm)
+    t = np.linspace(0, t_end, ntm)
+    xx, yy, zz = np.meshgrid(x, y, z, indexing="ij")
+    psi = (z0 - zz).reshape(-1, order="F")
+    nx = int(round(Lx / dxd))
+    ny = int(round(Ly / dxd))
+    alpha = voronoi_substrate(nx + 1, ny + 1, num_grains, seed, periodic)
+    theta = grain_angles(num_grains, seed)
+    uc = G * R * 1e6 * 1e-6  # K/us
+
+    def put(name, arr, fmt="%1.4e"):
+        np.savetxt(os.path.join(folder, name), np.asarray(arr).reshape(-1), fmt=fmt, delimiter="\n")
+
+    put("x.txt", x)
+    put("y.txt", y)
+    put("z.txt", z)
+    put("t.txt", t)
+    put("psi.txt", psi)
+    put("alpha.txt", alpha.reshape(-1), "%d")
+    put("theta.txt", theta)
+    put("G.txt", [G])
+    put("Rmax.txt", [R])
+    put("V.txt", [0.0])
+    put("Nmax.txt", [0.01])
+    put("UC.txt", [uc])
+    put("NG.txt", [num_grains], "%d")
+    put("NN.txt", [2 * num_grains], "%d")
+    put("z0.txt", [z0])
+    put("r0.txt", [0.9 * Lz])
+    put("x0.txt", [0.0])
+    put("top.txt", [top])
+    put("angle.txt", [0.0])
+    put("min_angle.txt", [0.0])
+    put("order.txt", [1.0])
+    return dict(nx=nx, ny=ny, alpha=alpha, theta=theta)

@@ -139,6 +139,18 @@ class APTSolver:
         abi.check(self.L.cupf_apt_time_steps(self.h, int(nsteps), C.byref(ms)))
         return ms.value
 
+    def nucl_init(self):
+        abi.check(self.L.cupf_apt_nucl_init(self.h))
+
+    def nucleate(self, use_initial_undercooling=False):
+        """One nucleation pass; returns the number of nuclei so far."""
+        n = C.c_int32()
+        abi.check(self.L.cupf_apt_nucleate(self.h, int(bool(use_initial_undercooling)), C.byref(n)))
+        return n.value
+
+    def nucl_reset(self):
+        abi.check(self.L.cupf_apt_nucl_reset(self.h))
+
     def set_tuning(self, z_chunk):
         abi.check(self.L.cupf_apt_set_tuning(self.h, int(z_chunk)))
 

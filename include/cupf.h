@@ -182,6 +182,29 @@ cupf_status cupf_apt_grain_volumes(cupf_apt_handle* h, int32_t num_grains,
  * no counterpart (its QoIs are integer voxel counts, QOI.cpp:38-231). */
 cupf_status cupf_apt_qoi_sums(cupf_apt_handle* h, double* out);
 
+/* ---------------------------------------------------------------- nucleation
+ * Coarse cells of (2*pts_cell+1)^3 fine cells (cnx = (fnx-3)/(2*pts_cell+1), ...)
+ * each hold a status (1 = solid or already nucleated).
+ * cupf_apt_nucl_init: status from slot 0 at each coarse cell's centre, indexed
+ *   without the halo offset exactly as init_nucl_status does
+ *   (3DgrainMPI/APTPhaseField.cu:420-444, 733-745).
+ * cupf_apt_nucleate: one add_nucl pass on the current state (:459-536, called
+ *   after the odd step of each evolve iteration, :866-870): a liquid coarse cell
+ *   nucleates with the reference's Gaussian probability (:446-455; undercooling
+ *   from the liquid-start rate when use_initial_undercooling, else from the 4-D
+ *   T_3D table), using time t = (steps done)*dt*tau0 and interval 2*dt*tau0.  The
+ *   draw is Philox4x32-10 keyed on (seed, coarse cell, step) instead of curand;
+ *   a nucleus is the (2*pts_cell+1)^3 tanh sphere in slot 0 with a new grain id
+ *   num_theta + 1 + (draw mod id_space), id_space = 2^30 (FP32) or
+ *   32767 - num_theta (16-bit storage).  *total (may be NULL) receives the
+ *   number of nuclei so far.
+ * cupf_apt_nucl_reset: every status to 0 (the reference's reset before the
+ *   liquid-start phase, :781). */
+cupf_status cupf_apt_nucl_init(cupf_apt_handle* h);
+cupf_status cupf_apt_nucleate(cupf_apt_handle* h, int32_t use_initial_undercooling,
+                              int32_t* total);
+cupf_status cupf_apt_nucl_reset(cupf_apt_handle* h);
+
 /* Moving-domain check and shift (line configuration).  Computes the per-layer
  * mean of phi over all slots and cells, advances *tip_front while the mean is
  * above LS, and while *tip_front >= tip_thres shifts the window down one layer:

@@ -507,3 +507,141 @@ void oracle_move_frame(const cupf_apt_params* p, float* PFs, int32_t* ids, float
   for (int k = 1; k < g.fnz - 2; ++k) z[k] = z[k + 1];
   z[g.fnz - 2] = ztop;
 }
+
+/* ---------------------------------------------------------------- nucleation
+ * add_nucl (APTPhaseField.cu:459-536) with the library's defined draw: Philox4x32-10
+ * (Salmon et al., SC 2011) keyed on (seed, coarse cell, step) instead of curand.
+ * Same probability (nuncl_possibility :446-455, evaluated in double), same table
+ * interpolation (interp4Dtemperature, devicefunc.cu_inl:32-83, separate roundings),
+ * same nucleus profile table and id rule as the CUDA kernel. */
+typedef struct { uint32_t v[4]; } philox4_t;
+
+static philox4_t philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
+                               uint32_t k1) {
+  for (int r = 0; r < 10; ++r) {
+    uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0, hi1 = (uint32_t)(p1 >> 32),
+             lo1 = (uint32_t)p1;
+    uint32_t n0 = hi1 ^ c1 ^ k0, n1 = lo1, n2 = hi0 ^ c3 ^ k1, n3 = lo0;
+    c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  philox4_t o = {{c0, c1, c2, c3}};
+  return o;
+}
+
+void oracle_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1,
+                   uint32_t* out) {
+  philox4_t r = philox4x32_10(c0, c1, c2, c3, k0, k1);
+  for (int i = 0; i < 4; ++i) out[i] = r.v[i];
+}
+
+static float uniform01(uint32_t x) { return (float)((x >> 8) + 1u) * (1.0f / 16777216.0f); }
+
+static float interp4d_f32(const float* u, float x, float y, float z, float t, int Nx, int Ny,
+                          int Nz, int Nt, float Dx, float Dt) {
+  float fx = x / Dx, fy = y / Dx, fz = z / Dx, ft = t / Dt;
+  int kx = (int)fx, ky = (int)fy, kz = (int)fz, kt = (int)ft;
+  float dx = fx - (float)kx, dy = fy - (float)ky, dz = fz - (float)kz, dtt = ft - (float)kt;
+  if (kx == Nx - 1) { kx = Nx - 2; dx = 1.0f; }
+  if (ky == Ny - 1) { ky = Ny - 2; dy = 1.0f; }
+  if (kz == Nz - 1) { kz = Nz - 2; dz = 1.0f; }
+  if (kt == Nt - 1) { kt = Nt - 2; dtt = 1.0f; }
+  if (kx < 0) kx = 0; if (kx > Nx - 2) kx = Nx - 2;
+  if (ky < 0) ky = 0; if (ky > Ny - 2) ky = Ny - 2;
+  if (kz < 0) kz = 0; if (kz > Nz - 2) kz = Nz - 2;
+  if (kt < 0) kt = 0; if (kt > Nt - 2) kt = Nt - 2;
+  int64_t sx = 1, sy = Nx, sz = (int64_t)Nx * Ny, st = sz * Nz;
+  float ex = 1.0f - dx, ey = 1.0f - dy;
+  float wa = ex * ey, wb = ex * dy, wc = dx * ey, wd = dx * dy;
+  int64_t o = kx + ky * sy + kz * sz + kt * st;
+  float q[4];
+  int64_t base[4] = {o, o + sz, o + st, o + st + sz};
+  for (int m = 0; m < 4; ++m) {
+    int64_t b = base[m];
+    float r = wa * u[b];
+    r = r + wb * u[b + sy];
+    r = r + wc * u[b + sx];
+    q[m] = r + wd * u[b + sy + sx];
+  }
+  float t0 = q[0] * (1.0f - dz) + q[1] * dz;
+  float t1 = q[2] * (1.0f - dz) + q[3] * dz;
+  return (1.0f - dtt) * t0 + dtt * t1;
+}
+
+static double nucl_probability(double delT, double d_delT, double nmax, double mean, double sd,
+                               double rad) {
+  double q = (delT - mean) / sd;
+  double density = nmax / (sqrt(2.0 * 3.14159265358979323846) * sd) * exp(-0.5 * q * q) * d_delT;
+  return 8.0 * rad * rad * rad * density;
+}
+
+int oracle_nucl_dims(const cupf_apt_params* p, int32_t* cdims) {
+  int w = 2 * p->pts_cell + 1;
+  cdims[0] = (p->fnx - 3) / w;
+  cdims[1] = (p->fny - 3) / w;
+  cdims[2] = (p->fnz - 3) / w;
+  return cdims[0] * cdims[1] * cdims[2];
+}
+
+/* init_nucl_status (APTPhaseField.cu:420-444), centre index without the halo offset */
+void oracle_nucl_status_init(const cupf_apt_params* p, const float* PFs, int32_t* status) {
+  int32_t cd[3];
+  oracle_nucl_dims(p, cd);
+  int w = 2 * p->pts_cell + 1;
+  for (int k = 0; k < cd[2]; ++k)
+    for (int j = 0; j < cd[1]; ++j)
+      for (int i = 0; i < cd[0]; ++i) {
+        int64_t g = (int64_t)(w * k + p->pts_cell) * p->fnx * p->fny +
+                    (int64_t)(w * j + p->pts_cell) * p->fnx + (w * i + p->pts_cell);
+        status[i + (int64_t)cd[0] * (j + (int64_t)cd[1] * k)] = ((double)PFs[g] > LS) ? 1 : 0;
+      }
+}
+
+/* One add_nucl pass; returns the number of new nuclei. */
+int oracle_nucleate(const cupf_apt_params* p, const cupf_apt_inputs* th, float* PFs, int32_t* ids,
+                    int32_t* status, const float* sphere, float t, float dt2, uint32_t step,
+                    int use_iuc, int id_space) {
+  int32_t cd[3];
+  oracle_nucl_dims(p, cd);
+  grid_t g = mkgrid(p);
+  int w = 2 * p->pts_cell + 1, pts = p->pts_cell, count = 0;
+  for (int64_t C = 0; C < (int64_t)cd[0] * cd[1] * cd[2]; ++C) {
+    if (status[C]) continue;
+    int i = (int)(C % cd[0]), j = (int)((C / cd[0]) % cd[1]), k = (int)(C / ((int64_t)cd[0] * cd[1]));
+    int gi = w * i + pts + 1, gj = w * j + pts + 1, gk = w * k + pts + 1;
+    int64_t gc = (int64_t)gk * g.fnx * g.fny + (int64_t)gj * g.fnx + gi;
+    int solid = 0;
+    for (int pf = 0; pf < g.np; ++pf) solid |= (double)PFs[gc + pf * g.len] > LS;
+    if (solid) { status[C] = 1; continue; }
+    double P;
+    if (use_iuc) {
+      float delT = (float)((double)p->underCoolingRate0 * 1e6 * (double)(t + dt2));
+      float d_delT = (float)((double)p->underCoolingRate0 * 1e6 * (double)dt2);
+      P = nucl_probability(delT, d_delT, p->nuc_Nmax0, p->undcool_mean, p->undcool_std, p->nuc_rad);
+    } else if (th->T_3D) {
+      float Dx = th->X_mac[1] - th->X_mac[0], Dt = th->t_mac[1] - th->t_mac[0];
+      float xq = th->x[gi] - th->X_mac[0], yq = th->y[gj] - th->Y_mac[0], zq = th->z[gk] - th->Z_mac[0];
+      float T0 = interp4d_f32(th->T_3D, xq, yq, zq, t - th->t_mac[0], p->Nx, p->Ny, p->Nz, p->Nt, Dx, Dt);
+      float T1 = interp4d_f32(th->T_3D, xq, yq, zq, (t + dt2) - th->t_mac[0], p->Nx, p->Ny, p->Nz, p->Nt, Dx, Dt);
+      P = nucl_probability(-T1, T0 - T1, p->nuc_Nmax, p->undcool_mean, p->undcool_std, p->nuc_rad);
+    } else {
+      continue;
+    }
+    philox4_t r = philox4x32_10((uint32_t)C, step, 0x4E55434Cu, 0u, (uint32_t)p->seed, 0x5EEDu);
+    if (!((double)uniform01(r.v[0]) < P)) continue;
+    int id = p->num_theta + 1 + (int)(r.v[1] % (uint32_t)id_space);
+    for (int dk = -pts; dk <= pts; ++dk)
+      for (int dj = -pts; dj <= pts; ++dj)
+        for (int di = -pts; di <= pts; ++di) {
+          float v = sphere[((dk + pts) * w + (dj + pts)) * w + (di + pts)];
+          int64_t o = gc + (int64_t)dk * g.fnx * g.fny + (int64_t)dj * g.fnx + di;
+          PFs[o] = v;
+          if (v > -0.9999f) ids[o] = id; /* float literal in add_nucl :524 */
+        }
+    status[C] = 1;
+    count++;
+  }
+  return count;
+}

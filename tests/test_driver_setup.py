@@ -1,0 +1,37 @@
+"""The C++ driver reads a forcing folder and input file the way the reference
+does (parseInputParams + cpuSetup + initField, PhaseFieldCpu.cpp:17-459) and
+arrives at the same parameters and initial state as the in-memory case builder
+(which restates the same derivation), up to the 5 significant digits the
+forcing files store."""
+import numpy as np
+
+from cupf_b200 import cases, host_api, preprocess
+
+
+def test_setup_from_forcing_folder(tmp_path, monkeypatch, built):
+    Lx, Ly, Lz = 2.48, 1.92, 2.48   # 32 x 25 x 32 interior points at dx*W0 = 0.08 um
+    z0 = 0.62
+    folder = tmp_path / "forcing" / "case3"
+    info = preprocess.write_line_forcing(str(folder), Lx, Ly, Lz, num_grains=9, seed=3, G=1.0,
+                                         R=0.05, z0=z0, top=0.4, t_end=1e-6)
+    preprocess.write_input_file(str(tmp_path / "line.py"), Lx, nts=2, asp_ratio_yx=Ly / Lx,
+                                asp_ratio_zx=2.0, moving_ratio=1.0, num_pf=5,
+                                extra={"kin_delta": 0.05})
+    monkeypatch.chdir(tmp_path)
+    dims, fp, phi, alpha = host_api.setup("line.py", str(folder), bc=(1, 1, 0), line_config=True)
+    assert tuple(dims) == (34, 27, 34, 9)
+    c = cases.line_case(32, 25, 32, num_pf=5, num_grains=9, seed=3, bc="110", z0_frac=z0 / Lz)
+    p = c.params
+    dt, tau0, lamd, hi, G, uc, z0r, kd = fp
+    assert dt == p.dt and tau0 == p.tau0 and lamd == p.lamd and hi == p.hi
+    assert abs(uc - 0.05) < 1e-6 and G == np.float32(1.0) and kd == np.float32(0.05)
+    # phi interpolated from the 5-digit macro grid vs the exact profile
+    inner = np.zeros((34, 27, 34), bool)
+    inner[1:-1, 1:-1, 1:-1] = True
+    inner = inner.reshape(-1)
+    assert np.max(np.abs(phi[inner] - c.phi[inner])) < 2e-3
+    # substrate ids where both are clearly solid
+    solid = inner & (c.phi > -0.99) & (phi > -0.99)
+    assert solid.sum() > 1000
+    assert np.array_equal(alpha[solid], c.alpha[solid])
+    assert np.all(alpha[inner & (phi <= -0.995)] == 0)
