@@ -35,6 +35,14 @@ struct PairF32 {
 
 enum class Half16 { BF16, FP16 };
 
+// 16-bit phi is stored as its distance to the nearest bulk value,
+//   u = copysign(1, phi) - phi,   phi = copysign(1, u) - u,
+// with u = +0 for phi = +1 and u = -0 for phi = -1 (empty slots stay exact).
+// A 16-bit float keeps ~11 (FP16) or 8 (BF16) significant bits of u, i.e.
+// relative precision of 1 - |phi| where the tanh profile's tails approach the
+// bulk values and change by less than a plain 16-bit spacing per step (plain
+// FP16 spacing is 4.9e-4 for |phi| in [0.5, 1): tails stall there).  Values
+// outside [-1, 1] (rounding overshoot) are stored as +-1.
 template <Half16 F>
 struct PairH16 {
   using T = uint32_t;
@@ -42,21 +50,24 @@ struct PairH16 {
   static constexpr int kBW = 36;  // 36*4 = 144 B (16 B multiple)
   static constexpr CUtensorMapDataType kTmaType = CU_TENSOR_MAP_DATA_TYPE_UINT32;
   static constexpr int kPitchAlign = 4;
-  __device__ static float phi(T p) {
-    const unsigned short b = (unsigned short)(p & 0xFFFFu);
-    if (F == Half16::BF16) return __bfloat162float(__ushort_as_bfloat16(b));
-    return __half2float(__ushort_as_half(b));
+  __device__ static float decode(unsigned short b) {
+    const float u = (F == Half16::BF16) ? __bfloat162float(__ushort_as_bfloat16(b))
+                                        : __half2float(__ushort_as_half(b));
+    return __fsub_rn(copysignf(1.0f, u), u);
   }
+  __device__ static unsigned short encode(float ph) {
+    // |u| = 1 - |phi| (exact for |phi| >= 0.5), clamped at 0, with phi's sign:
+    // phi = -1 gives -0, phi = +1 gives +0
+    const float u = copysignf(fmaxf(__fsub_rn(1.0f, fabsf(ph)), 0.0f), ph);
+    if (F == Half16::BF16) return __bfloat16_as_ushort(__float2bfloat16_rn(u));
+    return __half_as_ushort(__float2half_rn(u));
+  }
+  __device__ static float phi(T p) { return decode((unsigned short)(p & 0xFFFFu)); }
   __device__ static int id(T p) { return (int)(short)(p >> 16); }
   __device__ static T make(float ph, int id) {
-    unsigned short b;
-    if (F == Half16::BF16) b = __bfloat16_as_ushort(__float2bfloat16_rn(ph));
-    else b = __half_as_ushort(__float2half_rn(ph));
-    return (uint32_t)b | ((uint32_t)(unsigned short)(short)id << 16);
+    return (uint32_t)encode(ph) | ((uint32_t)(unsigned short)(short)id << 16);
   }
-  __device__ static T empty() {
-    return F == Half16::BF16 ? 0xFFFFBF80u : 0xFFFFBC00u;  // phi -1, id -1
-  }
+  __device__ static T empty() { return 0xFFFF8000u; }  // u = -0 (phi = -1), id -1
 };
 
 using PairBF16 = PairH16<Half16::BF16>;
