@@ -98,6 +98,8 @@ def lib():
             "cupf_apt_nucl_init": [vp],
             "cupf_apt_nucleate": [vp, C.c_int32, C.POINTER(C.c_int32)],
             "cupf_apt_nucl_reset": [vp],
+            "cupf_grain_volumes_noalloc": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                           C.POINTER(C.c_int64), vp],
             "cupf_server_create": [C.POINTER(cupf_server_config), C.POINTER(vp)],
             "cupf_server_destroy": [vp],
             "cupf_server_submit": [vp, C.POINTER(cupf_apt_params), C.POINTER(cupf_apt_inputs), FP,

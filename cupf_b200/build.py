@@ -17,7 +17,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 OUT = os.path.join(HERE, "libcupf.so")
 EXE = os.path.join(HERE, "phase_field")
 OBJ = os.path.join(HERE, "_build")
-CU_SOURCES = [os.path.join(HERE, "csrc", f) for f in ("cupf_capi.cu", "cupf_server.cu")]
+CU_SOURCES = [os.path.join(HERE, "csrc", f)
+              for f in ("cupf_capi.cu", "cupf_server.cu", "cupf_noalloc.cu")]
 CPP_SOURCES = [os.path.join(HERE, "host", f) for f in
                ("host_util.cpp", "qoi.cpp", "phase_field.cpp", "npz_writer.cpp", "host_capi.cpp")]
 MAIN = os.path.join(HERE, "host", "main.cpp")

@@ -205,6 +205,30 @@ cupf_status cupf_apt_nucleate(cupf_apt_handle* h, int32_t use_initial_undercooli
                               int32_t* total);
 cupf_status cupf_apt_nucl_reset(cupf_apt_handle* h);
 
+/* Allocation-free per-grain voxel counts (no counterpart in the reference).
+ * For callers that cannot let a library allocate device memory: codes that give
+ * all device memory to their own pool allocator at start-up, and services whose
+ * device footprint must stay fixed after start-up.  Same result as
+ * cupf_apt_grain_volumes (voxel count of every grain id 1..num_grains over the
+ * interior cells of an argmax map, counts[0] = interior cells with no such id),
+ * but the caller passes the argmax map alpha_dev (reference layout,
+ * fnx*fny*fnz int32, already in device memory) and a host array counts of
+ * num_grains+1 entries, and the call allocates nothing: its scratch is a fixed
+ * device array of CUPF_NOALLOC_MAX_GRAINS+1 counts and first-occurrence
+ * indices (1 MiB) that every GPU loading the library holds until the process
+ * exits.  num_grains above CUPF_NOALLOC_MAX_GRAINS is rejected
+ * (CUPF_ERR_INVALID).  Work is queued on `stream` (a cudaStream_t, NULL for
+ * the default stream) on the current device, and the call returns after the
+ * counts are in host memory.  The first call on a device looks up the scratch
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  Every call shares the one scratch array and clears it first, so
+ * calls whose GPU work overlaps (different streams or threads on one device)
+ * race and must be serialised by the caller. */
+#define CUPF_NOALLOC_MAX_GRAINS 65535
+cupf_status cupf_grain_volumes_noalloc(const int32_t* alpha_dev, int32_t fnx, int32_t fny,
+                                       int32_t fnz, int32_t num_grains, int64_t* counts,
+                                       void* stream);
+
 /* Moving-domain check and shift (line configuration).  Computes the per-layer
  * mean of phi over all slots and cells, advances *tip_front while the mean is
  * above LS, and while *tip_front >= tip_thres shifts the window down one layer:
