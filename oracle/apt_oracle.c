@@ -577,6 +577,19 @@ static double nucl_probability(double delT, double d_delT, double nmax, double m
   return 8.0 * rad * rad * rad * density;
 }
 
+/* Nucleus profile of add_nucl (APTPhaseField.cu:515-528): tanh(dx*((1+pts)/2 - r)/sqrt2)
+ * over the (2*pts+1)^3 cube, in float with the C library's tanhf. */
+void oracle_nucleus_table(const cupf_apt_params* p, float* out) {
+  const int pts = p->pts_cell, w = 2 * pts + 1;
+  const float pf = (float)pts;
+  for (int k = -pts; k <= pts; ++k)
+    for (int j = -pts; j <= pts; ++j)
+      for (int i = -pts; i <= pts; ++i) {
+        const float d = p->dx * ((1.0f + pf) / 2.0f - sqrtf((float)(i * i + j * j + k * k)));
+        out[((k + pts) * w + (j + pts)) * w + (i + pts)] = tanhf(d / p->sqrt2);
+      }
+}
+
 int oracle_nucl_dims(const cupf_apt_params* p, int32_t* cdims) {
   int w = 2 * p->pts_cell + 1;
   cdims[0] = (p->fnx - 3) / w;
