@@ -284,7 +284,13 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=40)
     ap.add_argument("--serve-precisions", default="fp32,fp16")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp16"])
+    ap.add_argument("--interior", type=int, nargs=3, metavar=("NX", "NY", "NZ"),
+                    help="smaller line case for profiling (grains scale with the xy area)")
     args = ap.parse_args()
+    if args.interior:
+        global INTERIOR, GRAINS
+        GRAINS = max(10, int(GRAINS * args.interior[0] * args.interior[1] / (INTERIOR[0] * INTERIOR[1])))
+        INTERIOR = tuple(args.interior)
     args.warmup = max(args.warmup, 3)
     ws, rank, local = dist_env()
     if args.impl == "reference":

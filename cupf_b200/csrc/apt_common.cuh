@@ -33,6 +33,7 @@ struct StepArgs {
   int ntx, nty, nzc, zc;  // tile grid and z-chunk length
   int num_theta, thermalType, use_iuc;
   float t;
+  uint32_t sr_key;  // per-step key of the stochastic-rounding bits (16-bit storage)
   float kin_delta, eps, G, z0, uc, uc0, L_cp, hi, lamd, dt, tau0;
   float lyd, lzd, r0, x0, angle, V, mp_len, order;
   int Nx, Ny, Nz;

@@ -333,6 +333,12 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
 #pragma unroll
     for (int q = 0; q < NP; ++q) phc[q] = (q < n) ? fetch(3, q) : -1.0f;
 
+    // rounding bits of this cell and step: keyed on the cell's reference-layout
+    // index and the step number, so a simulation rounds the same alone or batched
+    uint32_t cell_key = 0;
+    if (S::kStochastic)
+      cell_key = mix32((uint32_t)(gx + a.fnx * (gy + a.fny * k)) ^ mix32(a.sr_key));
+
     float Up = Up_plane;
     bool upd = true;
     if (!plane_T) {
@@ -375,7 +381,11 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
         for (int q = 0; q < NP; ++q)
           if (q != j && q < n) repul = repul_add(repul, phc[q]);
         const float nv = slot_update(a, ph7, sina, cosa, sinb, cosb, repul, Up);
-        o = S::make(nv, (nv < kDrop) ? -1 : id);  // (double)nv < -0.9999
+        const int oid = (nv < kDrop) ? -1 : id;  // (double)nv < -0.9999
+        if (S::kStochastic)
+          o = S::make_sr(nv, oid, mix32(cell_key + (uint32_t)j * 0x9E3779B9u));
+        else
+          o = S::make(nv, oid);
       }
       outp[j * ss] = o;
     }

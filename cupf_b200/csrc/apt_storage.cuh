@@ -2,7 +2,8 @@
 //
 // PairF32: the reference's own precision, {float phi, int32 id} in 8 bytes.
 // PairH16<F>: split precision, {16-bit phi, int16 id} in 4 bytes, phi in BF16
-//   or FP16 (round to nearest even on store); ids must fit in int16 (-1 = empty).
+//   or FP16 (the step stores with stochastic rounding, set-up paths round to
+//   nearest even); ids must fit in int16 (-1 = empty).
 // The step computes in FP32 for every format; only the stored pair differs.
 #pragma once
 
@@ -10,6 +11,7 @@
 #include <cuda_fp16.h>
 
 #include "apt_common.cuh"
+#include "rounding.cuh"
 
 namespace cupf {
 
@@ -31,6 +33,8 @@ struct PairF32 {
   __host__ __device__ static int id(T p) { return (int)p.y; }
   __device__ static T make(float ph, int id) { return make_uint2(__float_as_uint(ph), (uint32_t)id); }
   __device__ static T empty() { return make_uint2(0xBF800000u, 0xFFFFFFFFu); }
+  static constexpr bool kStochastic = false;
+  __device__ static T make_sr(float ph, int id, uint32_t) { return make(ph, id); }
 };
 
 enum class Half16 { BF16, FP16 };
@@ -61,6 +65,20 @@ struct PairH16 {
     const float u = copysignf(fmaxf(__fsub_rn(1.0f, fabsf(ph)), 0.0f), ph);
     if (F == Half16::BF16) return __bfloat16_as_ushort(__float2bfloat16_rn(u));
     return __half_as_ushort(__float2half_rn(u));
+  }
+  // Stochastic rounding of the step's output (r: 32 random bits): |u| goes to
+  // the 16-bit value below or above it with probabilities proportional to its
+  // distance from the other one, so the expected stored value equals the FP32
+  // result.  Round-to-nearest drops every per-step change smaller than half a
+  // 16-bit spacing, which biases slowly moving interfaces; this does not.
+  __device__ static unsigned short encode_sr(float ph, uint32_t r) {
+    const float u = copysignf(fmaxf(__fsub_rn(1.0f, fabsf(ph)), 0.0f), ph);
+    if (F == Half16::BF16) return sr_bf16_bits(u, r);
+    return sr_fp16_bits(u, r);
+  }
+  static constexpr bool kStochastic = true;
+  __device__ static T make_sr(float ph, int id, uint32_t r) {
+    return (uint32_t)encode_sr(ph, r) | ((uint32_t)(unsigned short)(short)id << 16);
   }
   __device__ static float phi(T p) { return decode((unsigned short)(p & 0xFFFFu)); }
   __device__ static int id(T p) { return (int)(short)(p >> 16); }

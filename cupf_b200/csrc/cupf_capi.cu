@@ -294,6 +294,19 @@ static void set_zc(cupf_apt_handle* h, int zc) {
   h->nzc = (nz + h->zc - 1) / h->zc;
 }
 
+// Default z-chunk of a work item: 16 planes (the best of 8..128 on the
+// 256x256x512 NUM_PF=8 line case), halved to 8 when that leaves fewer than
+// about eight items per resident CTA (two per SM), so that the heavy-first
+// schedule still has items to balance.
+static int default_zc(cupf_apt_handle* h) {
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+  const long long tiles = (long long)((h->p.fnx - 2 + TX - 1) / TX) * ((h->p.fny - 2 + TY - 1) / TY);
+  const int nz = h->p.fnz - 2;
+  if (tiles * ((nz + 15) / 16) < 8LL * 2 * nsm) return 8;
+  return 16;
+}
+
 static int grid_for(long long n, int block = 256) {
   long long b = (n + block - 1) / block;
   if (b > 148 * 16) b = 148 * 16;
@@ -397,7 +410,7 @@ extern "C" cupf_status cupf_apt_create(const cupf_apt_params* p, const cupf_apt_
   TRY(cuda(cudaMalloc((void**)&h->layer_sums, p->fnz * sizeof(double)), "layer sums"));
   for (int b = 0; b < 2; ++b) TRY(make_tmap(h, b));
   const char* zc_env = getenv("CUPF_ZC");
-  set_zc(h, zc_env ? atoi(zc_env) : 64);
+  set_zc(h, zc_env ? atoi(zc_env) : default_zc(h));
   TRY(cuda(cudaStreamSynchronize(h->stream), "sync"));
 #undef TRY
   *out = h;
@@ -510,6 +523,7 @@ extern "C" cupf_status cupf_apt_step(cupf_apt_handle* h, int32_t nsteps,
     // t of step m (1-based): (float)m * dt * tau0, as (2*kt+1)*dt*tau0 in evolve
     const float t = (float)(h->steps_done + 1) * h->p.dt * h->p.tau0;
     StepArgs a = step_args(h, t, use_initial_undercooling);
+    a.sr_key = (uint32_t)(h->steps_done + 1);
     a.in = h->buf[h->cur];
     a.out = h->buf[h->cur ^ 1];
     cupf_status st = launch_step(h, a, h->tmap[h->cur]);
