@@ -272,6 +272,101 @@ def run_serve(args):
     return 0
 
 
+EK2D_GRID = (2048, 8192)
+EK2D_STEPS = 50000
+EK2D_BYTES = {"fp64": 48, "fp32": 24, "fp16": 12, "bf16": 12}  # psi, U, dpsi read + written
+
+
+def ek2d_cpu_baseline(budget_s=15.0):
+    """FP64 oracle (OpenMP, all host threads) on a 512x2048 slab of the 2D case."""
+    from cupf_b200 import ek2d
+    from oracle import Ek2dOracle
+    c = ek2d.directional_case(512, 2048, 200, sites=8, amp=0.01)
+    o = Ek2dOracle()
+    s = o.new_state(c, np.float64)
+    o.run(c, s, 0, prestep=True)
+    steps, t_total = 0, 0.0
+    while t_total < budget_s and steps < 200:
+        t0 = time.perf_counter()
+        o.run(c, s, 5)
+        t_total += time.perf_counter() - t0
+        steps += 5
+    cells = 512 * 2049
+    return {"value": cells * steps / t_total / 1e6, "unit": "Mcell-upd/s", "cores": os.cpu_count(),
+            "kind": "port", "sample": "%d FP64 oracle steps of a 512x2048 slab (%.1f s)" % (steps, t_total)}
+
+
+def run_ek2d(args):
+    """Split-precision 2D Echebarria-Karma directional solidification: the full
+    run in FP64 (the error reference), FP32, FP16 and BF16 storage, each timed on
+    the device after `warmup` untimed steps; QoI errors against the FP64 run."""
+    from cupf_b200 import ek2d
+    nx, ny = EK2D_GRID if not args.ek2d_grid else tuple(args.ek2d_grid)
+    steps = args.ek2d_steps
+    warm = min(args.warmup, steps // 2)
+    case = ek2d.directional_case(nx, ny, steps, sites=32, amp=0.01)
+    p = case.params
+    dxd = float(p.dx) * float(p.W0)
+    q0 = ek2d.qois(case.phi, case.y64(), dxd)
+    cells = nx * (ny + 1)
+    res = {}
+    for prec in ("fp64", "fp32", "fp16", "bf16"):
+        with ek2d.EK2DSolver(case, precision=prec) as sv:
+            sv.set_state(case.psi, case.U)
+            sv.prestep()
+            sv.time_steps(warm)
+            with ClockSampler(0) as clk:
+                ms = sv.time_steps(steps - warm)
+            st = sv.get_state()
+            y = sv.get_y()
+            info = sv.info()
+        q = ek2d.qois(st["phi"], y, dxd)
+        per = ms / (steps - warm)
+        res[prec] = {"ms_per_step": per, "mcell_upd_per_s": cells / per / 1e3, "qois": q,
+                     "frame_shifts": info["shifts"], "clocks": clk.summary(),
+                     "hbm_gbs": EK2D_BYTES[prec] * cells / (per * 1e-3) / 1e9}
+    ref = res["fp64"]["qois"]
+    adv = ref["tip_y"] - q0["tip_y"]
+    for prec, r in res.items():
+        q = r["qois"]
+        r["tip_advance_rel_err"] = abs(q["tip_y"] - ref["tip_y"]) / abs(adv) if adv else None
+        r["tip_err_cells"] = abs(q["tip_y"] - ref["tip_y"]) / dxd
+        r["spacing_rel_err"] = (abs(q["spacing"] - ref["spacing"]) / ref["spacing"]
+                                if ref["spacing"] else None)
+    # end to end through the C ABI with host buffers: create, H2D of psi/U, the
+    # pre-step and all steps, D2H of the final fields
+    t0 = time.perf_counter()
+    with ek2d.EK2DSolver(case, precision="fp16") as sv:
+        sv.set_state(case.psi, case.U)
+        sv.prestep()
+        sv.step(steps)
+        st = sv.get_state()
+    e2e_s = time.perf_counter() - t0
+    head = res["fp16"]
+    peak, src = measured_peak()
+    out = {"metric": "2D EK Mcell-upd/s (split precision)", "value": head["mcell_upd_per_s"],
+           "unit": "Mcell-upd/s", "n_gpus": 1, "steps": steps - warm, "warmup": warm,
+           "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "fp16 storage, fp32 compute", "data": "synthetic",
+           "config": {"workload": "2D Echebarria-Karma directional solidification %dx%d, k=0.14, "
+                                  "G=0.1 K/um, R=1e4 um/s, 32 seeded sites +-0.01 W0, %d steps"
+                                  % (nx, ny, steps),
+                      "grid": [nx, ny], "dx_W0": float(p.dx), "W0_um": float(p.W0),
+                      "dt": float(p.dt), "l2": "fields 2x%.0f MB (fp16) per step" % (
+                          6 * (nx + 2) * (ny + 3) / 1e6)},
+           "roofline": {"bound": "hbm", "achieved": head["hbm_gbs"], "peak": peak, "unit": "GB/s",
+                        "frac": head["hbm_gbs"] / peak, "traffic": None, "peak_source": src,
+                        "algorithmic_bytes_per_cell": EK2D_BYTES["fp16"]},
+           "precisions": res,
+           "e2e": {"value": cells * steps / e2e_s / 1e6, "unit": "Mcell-upd/s",
+                   "h2d_bytes_per_step": 2 * 4 * case.fnx * case.fny / steps,
+                   "d2h_bytes_per_step": 4 * 4 * case.fnx * case.fny / steps, "seconds": e2e_s},
+           "cpu_baseline": None if args.no_cpu_baseline else ek2d_cpu_baseline(),
+           "clocks": head["clocks"], "gpu_launches": steps - warm}
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -286,6 +381,10 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp16"])
     ap.add_argument("--interior", type=int, nargs=3, metavar=("NX", "NY", "NZ"),
                     help="smaller line case for profiling (grains scale with the xy area)")
+    ap.add_argument("--workload", default="apt3d", choices=["apt3d", "ek2d"],
+                    help="ek2d: the split-precision 2D dendrite benchmark")
+    ap.add_argument("--ek2d-grid", type=int, nargs=2, metavar=("NX", "NY"))
+    ap.add_argument("--ek2d-steps", type=int, default=EK2D_STEPS)
     args = ap.parse_args()
     if args.interior:
         global INTERIOR, GRAINS
@@ -297,6 +396,8 @@ def main():
         return run_reference(args, ws, rank)
     if args.serve:
         return run_serve(args)
+    if args.workload == "ek2d":
+        return run_ek2d(args)
 
     import torch
     from cupf_b200.solver import APTSolver

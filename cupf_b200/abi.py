@@ -1,4 +1,4 @@
-"""ctypes mirror of include/cupf.h and the loader of the CUDA library.
+"""ctypes mirror of include/cupf.h, cupf_ek2d.h and the loader of the CUDA library.
 
 The library (cupf_b200/libcupf.so) is built in-tree by cupf_b200/build.py.
 Loading fails loudly when it is missing: there is no CPU fallback.
@@ -49,10 +49,29 @@ class cupf_server_config(C.Structure):
                 ("autotune", C.c_int32), ("hbm_budget_bytes", C.c_int64)]
 
 
+class cupf_ek2d_params(C.Structure):
+    """Parameters of the 2D Echebarria–Karma line model (include/cupf_ek2d.h)."""
+    _fields_ = ([(n, C.c_int32) for n in ("nx", "ny", "Mt", "seed_val", "tipp", "noi_period")] +
+                [("reserved_i", C.c_int32 * 2)] +
+                [(n, C.c_float) for n in (
+                    "G", "R", "delta", "k", "c_infm", "Dl", "d0", "W0", "c_infty", "eps", "alpha0",
+                    "dx", "asp_ratio", "lxd", "eta", "U0", "cfl",
+                    "lT", "lamd", "tau0", "R_tilde", "Dl_tilde", "lT_tilde", "dt", "lyd", "hi",
+                    "cosa", "sina", "sqrt2", "a_s", "epsilon", "a_12", "dt_sqrt", "blank", "ls")] +
+                [("y0", C.c_double), ("reserved_d", C.c_double * 3)])
+
+
+class cupf_ek2d_info(C.Structure):
+    _fields_ = [("steps", C.c_int64), ("shifts", C.c_int64), ("cur_tip", C.c_int32),
+                ("tip_thres", C.c_int32), ("t", C.c_double), ("intR", C.c_double),
+                ("lT_tilde", C.c_double)]
+
+
 STATUS = {0: "CUPF_OK", 1: "CUPF_ERR_INVALID", 2: "CUPF_ERR_CUDA", 3: "CUPF_ERR_OOM",
           4: "CUPF_ERR_UNSUPPORTED", 5: "CUPF_ERR_TIMEOUT", 6: "CUPF_ERR_IO", 7: "CUPF_ERR_STATE"}
 
 PREC = {"fp32": 0, "bf16": 1, "fp16": 2}
+PREC_EK2D = {"fp32": 0, "bf16": 1, "fp16": 2, "fp64": 3}
 
 
 class CupfError(RuntimeError):
@@ -110,6 +129,27 @@ def lib():
                                    C.POINTER(C.c_int64), C.c_int32, C.POINTER(C.c_double),
                                    C.POINTER(C.c_double)],
             "cupf_server_release": [vp, C.c_int64],
+            "cupf_ek2d_derive": [C.POINTER(cupf_ek2d_params), C.c_float],
+            "cupf_ek2d_parse_input": [C.c_char_p, C.POINTER(cupf_ek2d_params),
+                                      C.POINTER(C.c_int32), C.POINTER(C.c_int32), FP],
+            "cupf_ek2d_create": [C.POINTER(cupf_ek2d_params), C.c_int32, C.c_int32, C.POINTER(vp)],
+            "cupf_ek2d_destroy": [vp],
+            "cupf_ek2d_set_thermal": [vp, C.c_int32, FP, FP, FP],
+            "cupf_ek2d_set_state": [vp, FP, FP, FP],
+            "cupf_ek2d_prestep": [vp],
+            "cupf_ek2d_step": [vp, C.c_int32],
+            "cupf_ek2d_get_state": [vp, FP, FP, FP, FP],
+            "cupf_ek2d_get_state_f64": [vp] + [C.POINTER(C.c_double)] * 4,
+            "cupf_ek2d_get_y": [vp, C.POINTER(C.c_double)],
+            "cupf_ek2d_info_get": [vp, C.POINTER(cupf_ek2d_info)],
+            "cupf_ek2d_row_means": [vp, C.POINTER(C.c_double)],
+            "cupf_ek2d_time_steps": [vp, C.c_int32, FP],
+            "cupf_ek2d_stream": [vp, C.POINTER(vp)],
+            "cupf_host_ek2d_initial_fields": [C.POINTER(cupf_ek2d_params), C.c_int, FP, FP, FP, FP,
+                                              FP, FP, FP, FP],
+            "cupf_host_ek2d_perturb": [C.POINTER(cupf_ek2d_params), C.c_int, C.c_float, FP, FP],
+            "cupf_host_ek2d_qois": [FP, C.c_int, C.c_int, C.POINTER(C.c_double), C.c_double,
+                                    C.POINTER(C.c_double)],
         }.items():
             f = getattr(L, name)
             f.argtypes = args

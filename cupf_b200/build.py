@@ -16,12 +16,15 @@ ROOT = os.path.dirname(HERE)
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 OUT = os.path.join(HERE, "libcupf.so")
 EXE = os.path.join(HERE, "phase_field")
+EXE2D = os.path.join(HERE, "phase_field_2d")
 OBJ = os.path.join(HERE, "_build")
 CU_SOURCES = [os.path.join(HERE, "csrc", f)
-              for f in ("cupf_capi.cu", "cupf_server.cu", "cupf_noalloc.cu")]
+              for f in ("cupf_capi.cu", "cupf_server.cu", "cupf_noalloc.cu", "cupf_ek2d.cu")]
 CPP_SOURCES = [os.path.join(HERE, "host", f) for f in
-               ("host_util.cpp", "qoi.cpp", "phase_field.cpp", "npz_writer.cpp", "host_capi.cpp")]
+               ("host_util.cpp", "qoi.cpp", "phase_field.cpp", "npz_writer.cpp", "host_capi.cpp",
+                "ek2d_host.cpp")]
 MAIN = os.path.join(HERE, "host", "main.cpp")
+MAIN2D = os.path.join(HERE, "host", "ek2d_main.cpp")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
                   "--expt-relaxed-constexpr"]
@@ -33,8 +36,8 @@ def _deps():
     for sub in ("csrc", "host"):
         d = os.path.join(HERE, sub)
         hdrs += [os.path.join(d, f) for f in os.listdir(d) if f.endswith((".cuh", ".h"))]
-    return hdrs + [os.path.join(ROOT, "include", "cupf.h"),
-                   os.path.join(ROOT, "include", "cupf_host.h"), __file__]
+    return hdrs + [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))
+                   if f.endswith(".h")] + [__file__]
 
 
 def _newer(target, sources):
@@ -54,8 +57,8 @@ def _run(cmd, verbose=False):
 
 def build(force=False, verbose=False):
     deps = _deps()
-    allsrc = CU_SOURCES + CPP_SOURCES + [MAIN]
-    if not force and _newer(OUT, allsrc + deps) and _newer(EXE, allsrc + deps):
+    allsrc = CU_SOURCES + CPP_SOURCES + [MAIN, MAIN2D]
+    if not force and all(_newer(t, allsrc + deps) for t in (OUT, EXE, EXE2D)):
         return OUT
     os.makedirs(OBJ, exist_ok=True)
     jobs = []
@@ -66,18 +69,19 @@ def build(force=False, verbose=False):
         if force or not _newer(o, [s] + deps):
             jobs.append([NVCC] + NVFLAGS + (["-Xptxas", "-v"] if verbose else []) +
                         ["-c", s, "-o", o])
-    for s in CPP_SOURCES + [MAIN]:
+    for s in CPP_SOURCES + [MAIN, MAIN2D]:
         o = os.path.join(OBJ, os.path.basename(s) + ".o")
-        if s != MAIN:
+        if s not in (MAIN, MAIN2D):
             objs.append(o)
         if force or not _newer(o, [s] + deps):
             jobs.append(["g++"] + CXXFLAGS + ["-I", "/usr/local/cuda/include", "-c", s, "-o", o])
     with ThreadPoolExecutor(max_workers=8) as ex:
         list(ex.map(lambda c: _run(c, verbose), jobs))
     _run([NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart"])
-    _run(["g++", "-o", EXE, os.path.join(OBJ, "main.cpp.o"), "-L", HERE, "-lcupf",
-          "-Wl,-rpath,$ORIGIN", "-L/usr/local/cuda/lib64", "-lcudart",
-          "-Wl,-rpath,/usr/local/cuda/lib64"])
+    for exe, main in ((EXE, "main.cpp.o"), (EXE2D, "ek2d_main.cpp.o")):
+        _run(["g++", "-o", exe, os.path.join(OBJ, main), "-L", HERE, "-lcupf",
+              "-Wl,-rpath,$ORIGIN", "-L/usr/local/cuda/lib64", "-lcudart",
+              "-Wl,-rpath,/usr/local/cuda/lib64"])
     return OUT
 
 

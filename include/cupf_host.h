@@ -53,6 +53,31 @@ int cupf_host_setup(const char* input_file, const char* folder, int bcX, int bcY
                     int flags, int32_t* dims, float* fparams, float* phi, int32_t* alpha,
                     int64_t length_cap, char* err, int err_cap);
 
+/* 2D Echebarria–Karma line model (cupf_ek2d.h).  The params type is declared
+ * there; these take a pointer to it. */
+struct cupf_ek2d_params;
+
+/* Coordinates and initial fields of 2DdendriteMPI/line_model/main.cpp:225-271:
+ * x (fnx), y (fny), psi/phi/U (fnx*fny, reference layout, halos zero) from the
+ * 1-D profiles y_mac/psi_mac/U_mac of Ny points.  Any output may be NULL. */
+int cupf_host_ek2d_initial_fields(const struct cupf_ek2d_params* p, int Ny, const float* y_mac,
+                                  const float* psi_mac, const float* U_mac, float* x, float* y,
+                                  float* psi, float* phi, float* U);
+
+/* Seeded front perturbation (no counterpart in the reference): `sites`
+ * Gaussian bumps evenly spaced in x, each adding amp*(2u-1) to psi (u from
+ * Philox keyed on the site and seed_val); phi is recomputed. */
+int cupf_host_ek2d_perturb(const struct cupf_ek2d_params* p, int sites, float amp, float* psi,
+                           float* phi);
+
+/* Quantities of interest of one phi frame (FP64): out[0] tip height (highest
+ * phi = 0 crossing, um), out[1] mean column front height (um), out[2] primary
+ * spacing (um, 0 without cells), out[3] its wavenumber index, out[4] the row
+ * whose solid fraction is nearest 1/2 (-1 if none).  y holds the fny row
+ * coordinates, dxd the cell size in um. */
+int cupf_host_ek2d_qois(const float* phi, int fnx, int fny, const double* y, double dxd,
+                        double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,6 +9,9 @@ Outputs
                                 ...) compiled for sm_100a, NUM_PF=5 as shipped,
                                 with launchers (ref/ref_harness.cu)
   oracle/_ref/libref_aptN.so    the same with APT_NUM_PF set to N (N = 1..8)
+  oracle/_ref/libref_ek2d.so    reference 2D line-model kernels and setup()
+                                (2DdendriteMPI/line_model/PF.cu, unmodified) with
+                                launchers (ref/ref_ek2d_harness.cu)
 
 APTPhaseField.cu is compiled from a generated copy (oracle/_ref/srcN/, never
 committed) with exactly two textual edits:
@@ -33,6 +36,7 @@ from concurrent.futures import ThreadPoolExecutor
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 REF_DIR = os.environ.get("CUPF_REFERENCE_DIR", "/root/reference/3DgrainMPI")
+REF2D_DIR = os.environ.get("CUPF_REFERENCE_2D_DIR", "/root/reference/2DdendriteMPI/line_model")
 OUT = os.path.join(HERE, "_ref")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CUDA_INC = "/usr/local/cuda/include"
@@ -54,12 +58,13 @@ def _newer(target, sources):
 
 
 def build_oracle(force=False):
-    src = os.path.join(HERE, "apt_oracle.c")
+    srcs = [os.path.join(HERE, f) for f in ("apt_oracle.c", "ek2d_oracle.c")]
     out = os.path.join(HERE, "liboracle.so")
-    hdr = os.path.join(ROOT, "include", "cupf.h")
-    if force or not _newer(out, [src, hdr, __file__]):
-        _run(["gcc", "-O2", "-std=c11", "-fopenmp", "-ffp-contract=off", "-fPIC", "-shared",
-              src, "-o", out, "-lm"])
+    deps = srcs + [os.path.join(HERE, "ek2d_oracle_impl.h")] + [
+        os.path.join(ROOT, "include", f) for f in ("cupf.h", "cupf_ek2d.h")]
+    if force or not _newer(out, deps + [__file__]):
+        _run(["gcc", "-O2", "-std=c11", "-fopenmp", "-ffp-contract=off", "-fPIC", "-shared"] +
+             srcs + ["-o", out, "-lm"])
     return out
 
 
@@ -125,9 +130,28 @@ def build_ref_gpu(num_pf, force=False):
     return out
 
 
+def build_ref_ek2d(force=False):
+    """The reference's 2D line-model kernels (PF.cu, unmodified, from REF2D_DIR)
+    with the launchers of ref/ref_ek2d_harness.cu."""
+    if not os.path.isdir(REF2D_DIR):
+        return None
+    os.makedirs(OUT, exist_ok=True)
+    out = os.path.join(OUT, "libref_ek2d.so")
+    harness = os.path.join(HERE, "ref", "ref_ek2d_harness.cu")
+    deps = [harness, os.path.join(REF2D_DIR, "PF.cu"), os.path.join(ROOT, "include", "cupf_ek2d.h"),
+            __file__]
+    if not force and _newer(out, deps):
+        return out
+    _run([NVCC] + ARCH + ["-O3", "-std=c++14", "-w", "-Xcompiler", "-fPIC", "-lineinfo", "-shared",
+                          "-I", REF2D_DIR, harness, "-o", out, "-lcudart", "-Xlinker",
+                          "--no-undefined"])
+    return out
+
+
 def build_all(force=False):
     outs = [build_oracle(force)]
     outs.append(build_ref_host(force))
+    outs.append(build_ref_ek2d(force))
     with ThreadPoolExecutor(max_workers=2) as ex:
         outs += list(ex.map(lambda n: build_ref_gpu(n, force), range(1, 9)))
     return outs
