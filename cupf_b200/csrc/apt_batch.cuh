@@ -27,7 +27,7 @@ struct BatchSim {
 };
 
 template <int NP, class S>
-__global__ void __launch_bounds__(NTHREADS, 2)
+__global__ void __launch_bounds__(NTHREADS, step_min_blocks<NP, S>())
     apt_batch_step_kernel(BatchSim* sims, const CUtensorMap* tmaps, const int4* items, int nitems,
                           int* work) {
   extern __shared__ __align__(128) unsigned char smem[];

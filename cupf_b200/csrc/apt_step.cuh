@@ -237,6 +237,7 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
   const bool plane_T = a.use_iuc || a.thermalType == 0 || a.thermalType == 1;
   const float kLS = __uint_as_float(kLSFloatBits);
   const float kDrop = __uint_as_float(kDropFloatBits);
+  const KineConst kc = kine_const(a.kin_delta);
 
   for (int k = k_begin; k < k_end; ++k) {
     const int qk = k - k_begin + 1;
@@ -328,10 +329,16 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
       return S::phi(pts[s][cd * BCELLS]);
     };
 
-    // center values of every slot (for the repulsion sum)
+    // center values of every slot (for the repulsion sum); the loops over slots
+    // stop at n, so a warp runs only as many iterations as its fullest cell
     float phc[NP];
 #pragma unroll
-    for (int q = 0; q < NP; ++q) phc[q] = (q < n) ? fetch(3, q) : -1.0f;
+    for (int q = 0; q < NP; ++q) phc[q] = -1.0f;
+#pragma unroll
+    for (int q = 0; q < NP; ++q) {
+      if (q >= n) break;
+      phc[q] = fetch(3, q);
+    }
 
     // rounding bits of this cell and step: keyed on the cell's reference-layout
     // index and the step number, so a simulation rounds the same alone or batched
@@ -378,9 +385,11 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
         }
         float repul = 0.0f;
 #pragma unroll
-        for (int q = 0; q < NP; ++q)
-          if (q != j && q < n) repul = repul_add(repul, phc[q]);
-        const float nv = slot_update(a, ph7, sina, cosa, sinb, cosb, repul, Up);
+        for (int q = 0; q < NP; ++q) {
+          if (q >= n) break;
+          if (q != j) repul = repul_add(repul, phc[q]);
+        }
+        const float nv = slot_update(a, kc, ph7, sina, cosa, sinb, cosb, repul, Up);
         const int oid = (nv < kDrop) ? -1 : id;  // (double)nv < -0.9999
         if (S::kStochastic)
           o = S::make_sr(nv, oid, mix32(cell_key + (uint32_t)j * 0x9E3779B9u));
@@ -420,8 +429,15 @@ __device__ __forceinline__ int next_work_item(int* work, int nitems, int* s_item
 // nearest the bottom (the solid, where cells carry the most grain ids in a
 // directional-solidification run) start first and the light liquid chunks fill
 // in behind them.
+// Resident CTAs per SM the step is compiled for: three where three CTAs' shared
+// memory fits (16-bit pairs, or FP32 up to NUM_PF = 5), else two.
 template <int NP, class S>
-__global__ void __launch_bounds__(NTHREADS, 2)
+constexpr int step_min_blocks() {
+  return StepSmem<NP, S>::kBytes <= 74 * 1024 ? 3 : 2;
+}
+
+template <int NP, class S>
+__global__ void __launch_bounds__(NTHREADS, step_min_blocks<NP, S>())
     apt_step_kernel(const __grid_constant__ CUtensorMap tmap, const StepArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   CtaSmem<NP, S> sm(smem);

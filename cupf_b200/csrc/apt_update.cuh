@@ -36,12 +36,25 @@ __device__ __forceinline__ float sop(float x, float y, float u, float v) {
   return fadd(fmul(x, y), fmul(u, v));
 }
 
+// a_s = 1 + 3 kd and epsilon = -4 kd / a_s of kine_ani (APTPhaseField.cu:38-39),
+// which depend only on the launch's kin_delta: formed once per work item with
+// the same operations the reference repeats per call.
+struct KineConst {
+  float a_s, epsilon;
+};
+__device__ __forceinline__ KineConst kine_const(float kd) {
+  using K = Contract;
+  KineConst k;
+  k.a_s = K::AS ? ffma(3.0f, kd, 1.0f) : fadd(1.0f, fmul(3.0f, kd));
+  k.epsilon = __fdiv_rn(fmul(-4.0f, kd), k.a_s);
+  return k;
+}
+
 // 4-fold kinetic anisotropy of the rotated normal (APTPhaseField.cu:36-52).
 __device__ __forceinline__ float kine_ani(float ux, float uy, float uz, float cosa, float sina,
-                                          float cosb, float sinb, float kd, float eps) {
+                                          float cosb, float sinb, KineConst kc, float eps) {
   using K = Contract;
-  float a_s = K::AS ? ffma(3.0f, kd, 1.0f) : fadd(1.0f, fmul(3.0f, kd));
-  float epsilon = __fdiv_rn(fmul(-4.0f, kd), a_s);
+  const float a_s = kc.a_s, epsilon = kc.epsilon;
   float s = sop<K::UX_IN>(fmul(cosa, cosb), ux, fmul(sina, cosb), uy);
   float rx = K::UX_OUT ? ffma(-sinb, uz, s) : fsub(s, fmul(sinb, uz));
   float ry = fadd(sop<K::UY>(-sina, ux, cosa, uy), 0.0f);
@@ -133,16 +146,16 @@ __device__ __forceinline__ bool tinterp(const StepArgs& a, int i, int j, int k, 
 
 // New phi of one active slot (APTPhaseField.cu:254-340).  ph[0..6] are the
 // slot's values at D,B,L,C,R,T,U; repul the repulsion sum; Up = T/L_cp.
-__device__ __forceinline__ float slot_update(const StepArgs& a, const float ph[7], float sina,
-                                             float cosa, float sinb, float cosb, float repul,
-                                             float Up) {
+__device__ __forceinline__ float slot_update(const StepArgs& a, KineConst kc, const float ph[7],
+                                             float sina, float cosa, float sinb, float cosb,
+                                             float repul, float Up) {
   using K = Contract;
   const float phD = ph[0], phB = ph[1], phL = ph[2], phC = ph[3], phR = ph[4], phT = ph[5],
               phU = ph[6];
   float phx = fmul(fsub(phR, phL), 0.5f);
   float phy = fmul(fsub(phT, phB), 0.5f);
   float phz = fmul(fsub(phU, phD), 0.5f);
-  float A2 = kine_ani(phx, phy, phz, cosa, sina, cosb, sinb, a.kin_delta, a.eps);
+  float A2 = kine_ani(phx, phy, phz, cosa, sina, cosb, sinb, kc, a.eps);
   float sum = fadd(fadd(fadd(fadd(fadd(phR, phL), phT), phB), phU), phD);
   float diff = K::DIFF ? ffma(-6.0f, phC, sum) : fsub(sum, fmul(6.0f, phC));
   float w = K::W ? ffma(-phC, phC, 1.0f) : fsub(1.0f, fmul(phC, phC));

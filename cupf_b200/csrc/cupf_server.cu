@@ -411,10 +411,9 @@ static cupf_status rebuild(cupf_server* s) {
     s->dirty = false;
     return CUPF_OK;
   }
-  // persistent grid: 2 CTAs per SM, never more CTAs than items
+  // persistent grid: the resident CTAs of the step kernel, never more than items
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, s->cfg.device);
-  const int grid = std::min(s->nitems, 2 * nsm);
   const int nsims = (int)s->slots.size();
   cupf_status e = with_fmt(s->cfg.precision, [&](auto tag) -> cupf_status {
     using S = decltype(tag);
@@ -424,6 +423,10 @@ static cupf_status rebuild(cupf_server* s) {
     const int bytes = StepSmem<N, S>::kBytes;                                                \
     CK(cudaFuncSetAttribute(apt_batch_step_kernel<N, S>,                                     \
                             cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));            \
+    int per_sm = 2;                                                                          \
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, apt_batch_step_kernel<N, S>,   \
+                                                     NTHREADS, bytes));                      \
+    const int grid = std::min(s->nitems, std::max(1, per_sm) * nsm);                         \
     CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));                 \
     for (int k = 0; k < s->cfg.steps_per_round; ++k) {                                       \
       apt_batch_step_kernel<N, S><<<grid, NTHREADS, bytes, s->stream>>>(                     \
