@@ -42,7 +42,7 @@ TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "apt_step_c2_ncu.md")
 
 
 def workload_config(extra=None):
-    c = {"workload": "3D APT line step %dx%dx%d interior, NUM_PF=%d, %d grains, FP32 storage"
+    c = {"workload": "3D APT line step %dx%dx%d interior, NUM_PF=%d, %d grains"
                      % (*INTERIOR, NUM_PF, GRAINS),
          "interior": list(INTERIOR), "num_pf": NUM_PF, "grains": GRAINS, "seed": SEED,
          "bc": "110", "thermal": "line G=1 K/um R=0.05 m/s", "config_steps": CONFIG_STEPS,
@@ -414,7 +414,7 @@ def main():
     case = make_case()
     p = case.params
     cells = (p.fnx - 2) * (p.fny - 2) * (p.fnz - 2)
-    solver = APTSolver(case, device=device)
+    solver = APTSolver(case, precision=args.precision, device=device)
     solver.init_from_argmax(case.phi, case.alpha)
     solver.step(args.warmup)
     solver.sync()
@@ -435,7 +435,7 @@ def main():
     value = ws * cells * args.steps / (ms / 1e3) / 1e6
 
     # roofline of the step kernel (the only kernel in the timed region)
-    bytes_per_cell = 2 * NUM_PF * 8
+    bytes_per_cell = 2 * NUM_PF * (8 if args.precision == "fp32" else 4)
     launch_s = ms / 1e3 / args.steps
     achieved = cells * bytes_per_cell / launch_s / 1e9
     peak, peak_kind = measured_peak()
@@ -450,7 +450,7 @@ def main():
     if not args.no_e2e:
         barrier()
         t0 = time.perf_counter()
-        with APTSolver(case, device=device) as s2:
+        with APTSolver(case, precision=args.precision, device=device) as s2:
             s2.init_from_argmax(case.phi, case.alpha)
             s2.step(CONFIG_STEPS)
             phi, alpha = s2.collect(clear=True)
@@ -463,7 +463,7 @@ def main():
             e2e_s = float(t.item())
         L = case.length
         e2e = {"value": ws * cells * CONFIG_STEPS / e2e_s / 1e6, "unit": UNIT,
-               "h2d_bytes_per_step": (8 * L) / CONFIG_STEPS,
+               "h2d_bytes_per_step": (8 * L) / CONFIG_STEPS,  # phi + alpha, float32/int32
                "d2h_bytes_per_step": (8 * L + 8 * (GRAINS + 1)) / CONFIG_STEPS,
                "steps": CONFIG_STEPS, "seconds": e2e_s,
                "includes": "handle create + H2D phi/alpha + 2000 steps + argmax D2H + volumes"}
@@ -476,8 +476,11 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-                "config": workload_config({"parallelism": "replicas x%d" % ws}),
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "fp32" if args.precision == "fp32" else args.precision + " storage, fp32 compute",
+                "data": "synthetic",
+                "config": workload_config({"parallelism": "replicas x%d" % ws,
+                                           "storage": args.precision}),
                 "hbm_gbs": achieved, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "clocks": clk.summary(), "gpu_launches": args.steps,
                 "baseline_metric": "3D APT Mcell-upd/s & HBM GB/s, mixed vs FP32; served sims/hr,"

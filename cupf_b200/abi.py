@@ -117,6 +117,11 @@ def lib():
             "cupf_apt_nucl_init": [vp],
             "cupf_apt_nucleate": [vp, C.c_int32, C.POINTER(C.c_int32)],
             "cupf_apt_nucl_reset": [vp],
+            "cupf_apt_junction_candidates": [vp, C.POINTER(C.c_int64), C.c_int64,
+                                             C.POINTER(C.c_int64), C.POINTER(C.c_uint8)],
+            "cupf_host_junctions_3d_cells": [C.c_int] * 3 + [C.POINTER(C.c_int32),
+                                             C.POINTER(C.c_int64), C.c_int64,
+                                             C.POINTER(C.c_uint8), C.POINTER(C.c_int32), C.c_int],
             "cupf_grain_volumes_noalloc": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                            C.POINTER(C.c_int64), vp],
             "cupf_server_create": [C.POINTER(cupf_server_config), C.POINTER(vp)],

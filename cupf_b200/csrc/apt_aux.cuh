@@ -239,6 +239,56 @@ static __global__ void volume_kernel(const int* __restrict__ alpha, int fnx, int
   }
 }
 
+// Candidate cells of the 3D junction search (QOI3D::searchJunctionsOnImage,
+// QOI.cpp:233-311): a solid cell (alpha != 0) whose 19-point neighbourhood
+// (offsets with di^2 + dj^2 + dk^2 <= 2, itself included) holds no liquid cell,
+// exactly four distinct grain ids and no id more than ten times.  The indices
+// (reference layout) are appended in arbitrary order; `count` receives how many
+// cells qualify even past `cap`.  `distinct[idx]` (interior cells in (k, j, i)
+// order) receives the number of distinct values, liquid included, that the
+// reference's scan inserts into its hash map at that cell (0 where alpha == 0):
+// the host needs their running maximum to reproduce the map's bucket count,
+// which fixes the order of the grain ids in each record.
+static __global__ void junction_candidates_kernel(const int* __restrict__ alpha, int fnx, int fny,
+                                                  int fnz, long long* out, long long cap,
+                                                  unsigned long long* count,
+                                                  unsigned char* distinct) {
+  const long long ni = fnx - 2, nj = fny - 2, nk = fnz - 2;
+  const long long total = ni * nj * nk, plane = (long long)fnx * fny;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long i = 1 + idx % ni, j = 1 + (idx / ni) % nj, k = 1 + idx / (ni * nj);
+    const long long C = k * plane + j * fnx + i;
+    if (alpha[C] == 0) {
+      distinct[idx] = 0;
+      continue;
+    }
+    int vals[19], cnt[19];
+    int nd = 0, maxc = 0;
+    bool zero = false;
+    for (int dk = -1; dk <= 1; ++dk)
+      for (int dj = -1; dj <= 1; ++dj)
+        for (int di = -1; di <= 1; ++di) {
+          if (di * di + dj * dj + dk * dk > 2) continue;
+          const int v = alpha[C + dk * plane + dj * fnx + di];
+          zero |= (v == 0);
+          int f = -1;
+          for (int q = 0; q < nd; ++q)
+            if (vals[q] == v) f = q;
+          if (f < 0) {
+            vals[nd] = v;
+            cnt[nd] = 0;
+            f = nd++;
+          }
+          maxc = max(maxc, ++cnt[f]);
+        }
+    distinct[idx] = (unsigned char)nd;
+    if (zero || nd != 4 || maxc > 10) continue;
+    const unsigned long long slot = atomicAdd(count, 1ull);
+    if ((long long)slot < cap) out[slot] = C;
+  }
+}
+
 // FP64 interface QoIs over the interior, from m = max-over-slots phi of each cell:
 //   part[2*b]   = sum (1 + m) / 2              (solid volume, cell units)
 //   part[2*b+1] = sum |grad m| / 2             (interface area, cell units; a

@@ -102,6 +102,10 @@ struct cupf_apt_handle {
   unsigned long long* counts = nullptr;
   long long* first = nullptr;
   double* qoi_part = nullptr;
+  long long* jcand = nullptr;  // junction candidate cells
+  long long jcand_cap = 0;
+  unsigned long long* jcount = nullptr;
+  unsigned char* jdistinct = nullptr;  // distinct values per interior cell
   // nucleation
   int* nucl_status = nullptr;
   int* nucl_count = nullptr;
@@ -183,7 +187,7 @@ static void free_handle(cupf_apt_handle* h) {
                   h->Z_mac, h->t_mac, h->psi_mac, h->T_3D, h->phi_m, h->alpha_m, h->err, h->work,
                   h->xfer_ph, h->xfer_id, h->layer_sums, h->alpha_full, h->loss_area,
                   h->counts, h->first, h->qoi_part, h->nucl_status, h->nucl_count,
-                  h->nucl_sphere};
+                  h->nucl_sphere, h->jcand, h->jcount, h->jdistinct};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -560,6 +564,43 @@ extern "C" cupf_status cupf_apt_collect(cupf_apt_handle* h, int32_t clear, float
     CK(cudaMemcpyAsync(alpha_out, h->alpha_m, L * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   return check_err_word(h);
+}
+
+extern "C" cupf_status cupf_apt_junction_candidates(cupf_apt_handle* h, int64_t* cells,
+                                                    int64_t cap, int64_t* count,
+                                                    uint8_t* distinct) {
+  if (!h || !count || cap < 0 || (cap > 0 && !cells)) return fail(CUPF_ERR_INVALID, "bad argument");
+  if (!h->initialised) return fail(CUPF_ERR_STATE, "state not initialised");
+  CK(cudaSetDevice(h->device));
+  const Grid& g = h->g;
+  const long long ni = (long long)(g.fnx - 2) * (g.fny - 2) * (g.fnz - 2);
+  const long long want = cap > 0 ? cap : 1;
+  if (h->jcand_cap < want) {
+    if (h->jcand) cudaFree(h->jcand);
+    h->jcand = nullptr;
+    h->jcand_cap = 0;
+    CK(cudaMalloc((void**)&h->jcand, want * sizeof(long long)));
+    h->jcand_cap = want;
+  }
+  if (!h->jcount) CK(cudaMalloc((void**)&h->jcount, sizeof(unsigned long long)));
+  if (!h->jdistinct) CK(cudaMalloc((void**)&h->jdistinct, (size_t)ni));
+  CK(cudaMemsetAsync(h->jcount, 0, sizeof(unsigned long long), h->stream));
+  junction_candidates_kernel<<<grid_for(ni), 256, 0, h->stream>>>(
+      h->alpha_m, g.fnx, g.fny, g.fnz, h->jcand, cap, h->jcount, h->jdistinct);
+  CK(cudaGetLastError());
+  unsigned long long n = 0;
+  CK(cudaMemcpyAsync(&n, h->jcount, sizeof(n), cudaMemcpyDeviceToHost, h->stream));
+  if (distinct)
+    CK(cudaMemcpyAsync(distinct, h->jdistinct, (size_t)ni, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  const long long got = std::min<long long>((long long)n, cap);
+  if (got > 0) {
+    CK(cudaMemcpyAsync(cells, h->jcand, got * sizeof(long long), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    std::sort(cells, cells + got);
+  }
+  *count = (int64_t)n;
+  return CUPF_OK;
 }
 
 extern "C" cupf_status cupf_apt_grain_volumes(cupf_apt_handle* h, int32_t num_grains,

@@ -68,6 +68,23 @@ extern "C" int cupf_host_junctions_3d(int fnx, int fny, int fnz, const int32_t* 
   return n;
 }
 
+extern "C" int cupf_host_junctions_3d_cells(int fnx, int fny, int fnz, const int32_t* alpha,
+                                            const int64_t* cells, int64_t ncells,
+                                            const uint8_t* distinct, int32_t* nodes, int cap) {
+  QoiGrid g;
+  g.fnx = fnx;
+  g.fny = fny;
+  g.fnz = fnz;
+  QOI3D q(g);
+  q.calculateQoIs(g, alpha, 0);
+  std::vector<long long> c(cells, cells + ncells);
+  q.searchJunctionsOnCells(g, alpha, c.data(), ncells, distinct);
+  const std::vector<int>& v = q.mQoIVectorIntData["node_region"];
+  const int n = (int)v.size();
+  for (int i = 0; i < n && i < cap; ++i) nodes[i] = v[i];
+  return n;
+}
+
 extern "C" int cupf_host_get_param_float(const char* line, const char* key, float* value) {
   return getParam(std::string(line), std::string(key), *value) ? 1 : 0;
 }

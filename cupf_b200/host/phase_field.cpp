@@ -368,8 +368,16 @@ bool PhaseField::OutputQoIs() {
   const DesignSettingData* ds = GetSetDesignSetting();
   if (!qois) return setErr("no QoI object");
   const QoiGrid g = qoiGrid();
-  if (ds->useLineConfig) qois->searchJunctionsOnImage(g, alpha_i_full.data());
-  else qois->searchJunctionsOnImage(g, alpha.data());
+  std::vector<long long> cells;
+  std::vector<unsigned char> distinct;
+  QOI3D* q3 = dynamic_cast<QOI3D*>(qois.get());
+  if (ds->useLineConfig)
+    qois->searchJunctionsOnImage(g, alpha_i_full.data());
+  else if (q3 && deviceJunctionCandidates(cells, distinct))
+    q3->searchJunctionsOnCells(g, alpha.data(), cells.data(), (long long)cells.size(),
+                               distinct.data());
+  else
+    qois->searchJunctionsOnImage(g, alpha.data());
   const std::string name = outputBaseName() + "_walltime" + std::to_string(params.walltime) +
                            "_frames" + std::to_string(params.nts) + "_Mt" +
                            std::to_string(params.Mt) + "_rank0";
@@ -487,6 +495,25 @@ bool APTPhaseField::cudaSetup() {
   in.psi_mac = mac.psi_mac.data();
   in.T_3D = mac.T_3D.data();
   return check(cupf_apt_create(&d, &in, device, precision, &mHandle), "cupf_apt_create");
+}
+
+// The 19-point neighbourhood test of QOI3D::searchJunctionsOnImage on the device,
+// over the argmax map of the last collect (the map `alpha` holds).
+bool APTPhaseField::deviceJunctionCandidates(std::vector<long long>& cells,
+                                             std::vector<unsigned char>& distinct) {
+  if (!mHandle) return false;
+  distinct.assign((size_t)(fnx - 2) * (fny - 2) * (fnz - 2), 0);
+  int64_t cap = 1 << 16, count = 0;
+  for (;;) {
+    cells.assign((size_t)cap, 0);
+    if (cupf_apt_junction_candidates(mHandle, reinterpret_cast<int64_t*>(cells.data()), cap, &count,
+                                     distinct.data()) != CUPF_OK)
+      return false;
+    if (count <= cap) break;
+    cap = count;
+  }
+  cells.resize((size_t)count);
+  return true;
 }
 
 bool APTPhaseField::collectToHost(bool clear) {

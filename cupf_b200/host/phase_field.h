@@ -100,6 +100,11 @@ class PhaseField {
   bool initField();
   virtual bool cudaSetup() = 0;
   virtual bool evolve() = 0;
+  // Device candidates of the 3D junction search on the last collected argmax map
+  // (cells ascending, per-cell distinct counts); false where there are none.
+  virtual bool deviceJunctionCandidates(std::vector<long long>&, std::vector<unsigned char>&) {
+    return false;
+  }
   bool OutputQoIs();
   bool OutputField(int currentStep);
   void SetDesignSetting(const DesignSettingData* d) { mDesignSetting = d; }
@@ -130,6 +135,8 @@ class APTPhaseField : public PhaseField {
   ~APTPhaseField() override;
   bool cudaSetup() override;
   bool evolve() override;
+  bool deviceJunctionCandidates(std::vector<long long>& cells,
+                                std::vector<unsigned char>& distinct) override;
   cupf_apt_handle* handle() const { return mHandle; }
   cupf_apt_params deviceParams() const;
   int device = 0;

@@ -148,49 +148,94 @@ void QOI::calculateQoIs(const QoiGrid& g, const int* alpha, int /*kt*/) {
 
 // QOI3D::searchJunctionsOnImage (QOI.cpp:233-311): solid cells whose
 // 19-point neighbourhood (|d|^2 <= 2) holds no liquid and exactly 4 grains.
+// The junction record of one cell, or false when the cell is not a junction of
+// four grains (the body of the reference's scan, QOI.cpp:244-305).
+bool QOI3D::junctionRecord(const QoiGrid& g, const int* alpha, long long C,
+                           std::unordered_map<int, int>& occur, int* rec) const {
+  const int fnx = g.fnx, fny = g.fny;
+  if (alpha[C] == 0) return false;
+  occur.clear();
+  int zeros = 0;
+  for (int dk = -1; dk <= 1; ++dk)
+    for (int dj = -1; dj <= 1; ++dj)
+      for (int di = -1; di <= 1; ++di) {
+        if (di * di + dj * dj + dk * dk > 2) continue;
+        const int v = alpha[C + (long long)dk * fnx * fny + (long long)dj * fnx + di];
+        if (v == 0) zeros++;
+        auto it = occur.find(v);
+        if (it != occur.end())
+          it->second++;
+        else
+          occur.insert({v, 1});
+      }
+  if (zeros > 0) return false;
+  int n_alpha = 0, max_occ = 0;
+  for (auto& it : occur) {
+    n_alpha++;
+    max_occ = std::max(max_occ, it.second);
+  }
+  if (n_alpha != 4 || max_occ > 10) return false;
+  const long long plane = (long long)fnx * fny;
+  std::fill(rec, rec + mNumNodeFeatures, -1);  // unused features stay -1
+  rec[0] = (int)(C % fnx);
+  rec[1] = (int)((C / fnx) % fny);
+  rec[2] = (int)(C / plane);
+  rec[3] = max_occ;
+  int c = 0;
+  for (auto& it : occur) rec[4 + c++] = it.first;
+  return true;
+}
+
 void QOI3D::searchJunctionsOnImage(const QoiGrid& g, const int* alpha) {
-  const int fnx = g.fnx, fny = g.fny, fnz = g.fnz;
   std::vector<int>& node = mQoIVectorIntData["node_region"];
   node.assign((size_t)40 * mNumActiveGrains * mNumNodeFeatures, -1);
   size_t node_cnt = 0;
   std::unordered_map<int, int> occur;
-  for (int k = 1; k < fnz - 1; ++k)
-    for (int j = 1; j < fny - 1; ++j)
-      for (int i = 1; i < fnx - 1; ++i) {
-        const long long C = (long long)k * fnx * fny + (long long)j * fnx + i;
-        if (alpha[C] == 0) continue;
-        occur.clear();
-        int zeros = 0;
-        for (int dk = -1; dk <= 1; ++dk)
-          for (int dj = -1; dj <= 1; ++dj)
-            for (int di = -1; di <= 1; ++di) {
-              if (di * di + dj * dj + dk * dk > 2) continue;
-              const int v = alpha[(long long)(k + dk) * fnx * fny + (long long)(j + dj) * fnx + i + di];
-              if (v == 0) zeros++;
-              auto it = occur.find(v);
-              if (it != occur.end())
-                it->second++;
-              else
-                occur.insert({v, 1});
-            }
-        if (zeros > 0) continue;
-        int n_alpha = 0, max_occ = 0;
-        for (auto& it : occur) {
-          n_alpha++;
-          max_occ = std::max(max_occ, it.second);
-        }
-        if (n_alpha == 4 && max_occ <= 10) {
-          if ((node_cnt + 1) * mNumNodeFeatures > node.size()) continue;
-          const size_t o = node_cnt * mNumNodeFeatures;
-          node[o] = i;
-          node[o + 1] = j;
-          node[o + 2] = k;
-          node[o + 3] = max_occ;
-          int c = 0;
-          for (auto& it : occur) node[o + 4 + c++] = it.first;
-          node_cnt++;
-        }
+  int rec[9];
+  for (int k = 1; k < g.fnz - 1; ++k)
+    for (int j = 1; j < g.fny - 1; ++j)
+      for (int i = 1; i < g.fnx - 1; ++i) {
+        const long long C = (long long)k * g.fnx * g.fny + (long long)j * g.fnx + i;
+        if (!junctionRecord(g, alpha, C, occur, rec)) continue;
+        if ((node_cnt + 1) * mNumNodeFeatures > node.size()) continue;
+        std::copy(rec, rec + mNumNodeFeatures, node.begin() + node_cnt * mNumNodeFeatures);
+        node_cnt++;
       }
+}
+
+// The same records from the device's candidate list (ascending) and the
+// per-cell distinct-value counts of the full scan.  The scan above reuses one
+// hash map, cleared per cell; its bucket count only grows, with the largest
+// number of values any earlier cell inserted, and fixes the order in which a
+// record lists its grain ids.  Before each candidate the map is grown to the
+// running maximum of those counts (filling it with that many keys and clearing
+// it), so every record comes out as the full scan writes it.
+void QOI3D::searchJunctionsOnCells(const QoiGrid& g, const int* alpha, const long long* cells,
+                                   long long ncells, const unsigned char* distinct) {
+  std::vector<int>& node = mQoIVectorIntData["node_region"];
+  node.assign((size_t)40 * mNumActiveGrains * mNumNodeFeatures, -1);
+  size_t node_cnt = 0;
+  std::unordered_map<int, int> occur;
+  int rec[9];
+  const long long ni = g.fnx - 2, nj = g.fny - 2, plane = (long long)g.fnx * g.fny;
+  long long scanned = 0;  // interior cells folded into running_max so far
+  int running_max = 0, grown = 0;
+  for (long long n = 0; n < ncells; ++n) {
+    const long long C = cells[n];
+    const long long k = C / plane, j = (C / g.fnx) % g.fny, i = C % g.fnx;
+    const long long idx = (k - 1) * ni * nj + (j - 1) * ni + (i - 1);
+    for (; scanned <= idx; ++scanned) running_max = std::max(running_max, (int)distinct[scanned]);
+    if (running_max > grown) {
+      occur.clear();
+      for (int v = 0; v < running_max; ++v) occur.insert({v, 0});
+      occur.clear();
+      grown = running_max;
+    }
+    if (!junctionRecord(g, alpha, C, occur, rec)) continue;
+    if ((node_cnt + 1) * mNumNodeFeatures > node.size()) continue;
+    std::copy(rec, rec + mNumNodeFeatures, node.begin() + node_cnt * mNumNodeFeatures);
+    node_cnt++;
+  }
 }
 
 }  // namespace cupf_host

@@ -10,6 +10,7 @@
 
 #include <map>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 namespace cupf_host {
@@ -48,8 +49,14 @@ class QOI3D : public QOI {
  public:
   explicit QOI3D(const QoiGrid& g);
   void searchJunctionsOnImage(const QoiGrid& g, const int* alpha) override;
+  // The same records from the device's ascending candidate list and per-cell
+  // distinct-value counts (cupf_apt_junction_candidates).
+  void searchJunctionsOnCells(const QoiGrid& g, const int* alpha, const long long* cells,
+                              long long ncells, const unsigned char* distinct);
 
  private:
+  bool junctionRecord(const QoiGrid& g, const int* alpha, long long C,
+                      std::unordered_map<int, int>& occur, int* rec) const;
   int mNumNodeFeatures = 9;
 };
 

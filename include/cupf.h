@@ -205,6 +205,20 @@ cupf_status cupf_apt_nucleate(cupf_apt_handle* h, int32_t use_initial_undercooli
                               int32_t* total);
 cupf_status cupf_apt_nucl_reset(cupf_apt_handle* h);
 
+/* Candidate cells of the 3D junction search (QOI3D::searchJunctionsOnImage,
+ * QOI.cpp:233-311), on the device, over the argmax map of the last
+ * cupf_apt_collect: solid cells whose 19-point neighbourhood has no liquid cell,
+ * exactly four grain ids and no id more than ten times.  Writes up to `cap`
+ * cell indices (reference layout) in ascending order and the number of
+ * candidates to *count (which can exceed cap: call again with more room).
+ * `distinct` (may be NULL; (fnx-2)*(fny-2)*(fnz-2) bytes, interior cells in
+ * (k, j, i) order) receives each cell's number of distinct neighbourhood values,
+ * which the host needs to list each junction's grain ids in the reference's
+ * order.  Building the records of the candidate cells only
+ * (cupf_host_junctions_3d_cells) gives the records of the full host scan. */
+cupf_status cupf_apt_junction_candidates(cupf_apt_handle* h, int64_t* cells, int64_t cap,
+                                         int64_t* count, uint8_t* distinct);
+
 /* Allocation-free per-grain voxel counts (no counterpart in the reference).
  * For callers that cannot let a library allocate device memory: codes that give
  * all device memory to their own pool allocator at start-up, and services whose

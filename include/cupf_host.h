@@ -33,6 +33,12 @@ int cupf_host_sample_heights(int* cur_tip, const int32_t* alpha, int fnx, int fn
  * returns the record length used (40 * active grains * 9). */
 int cupf_host_junctions_3d(int fnx, int fny, int fnz, const int32_t* alpha, int32_t* nodes, int cap);
 
+/* The same records from the device's junction candidates: `cells` (ascending)
+ * and `distinct` as cupf_apt_junction_candidates returns them. */
+int cupf_host_junctions_3d_cells(int fnx, int fny, int fnz, const int32_t* alpha,
+                                 const int64_t* cells, int64_t ncells, const uint8_t* distinct,
+                                 int32_t* nodes, int cap);
+
 /* getParam (helper.cpp:44-74); returns 1 if the key was set. */
 int cupf_host_get_param_float(const char* line, const char* key, float* value);
 int cupf_host_get_param_int(const char* line, const char* key, int32_t* value);
