@@ -22,6 +22,7 @@ struct cupf_ek2d_handle {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int fnx = 0, fny = 0, pitch = 0;
+  int rows = 32;  // rows per warp of the step kernel
   long long plane = 0;
   size_t vbytes = 4;
   void* buf[2] = {nullptr, nullptr};
@@ -110,19 +111,25 @@ EkArgs make_args(const cupf_ek2d_handle* h, int prestep, uint32_t step) {
   return a;
 }
 
+// Rows each warp marches over: 32, halved (down to 8) while the grid would give
+// fewer than about two waves of resident warps (32 per SM at 8 warps per CTA).
+int march_rows(const cupf_ek2d_handle* h) {
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+  const long long strips = (h->fnx - 2 + MW - 1) / MW;
+  int rows = 32;
+  while (rows > 8 && strips * ((h->fny - 2 + rows - 1) / rows) < 2LL * 32 * nsm) rows /= 2;
+  return rows;
+}
+
 cupf_status launch_step(cupf_ek2d_handle* h, int prestep, uint32_t step) {
-  const EkArgs a = make_args(h, prestep, step);
-  const dim3 grid((h->fnx - 2 + TW - 1) / TW, (h->fny - 2 + TH - 1) / TH);
+  EkArgs a = make_args(h, prestep, step);
+  a.rows = h->rows;
+  const int nstrips = (h->fnx - 2 + MW - 1) / MW;
+  const dim3 grid((nstrips + MWARPS - 1) / MWARPS, (h->fny - 2 + a.rows - 1) / a.rows);
   return with_ek_storage(h->prec, [&](auto tag) -> cupf_status {
     using S = decltype(tag);
-    using T = typename S::T;
-    const int bytes = (int)sizeof(Tile<T>);
-    static bool attr_set[64] = {false};
-    if (!attr_set[h->device & 63]) {
-      CK(cudaFuncSetAttribute(ek2d_step_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-      attr_set[h->device & 63] = true;
-    }
-    ek2d_step_kernel<S><<<grid, NTHREADS, bytes, h->stream>>>(a);
+    ek2d_march_kernel<S><<<grid, MWARPS * 32, 0, h->stream>>>(a);
     CK(cudaGetLastError());
     return CUPF_OK;
   });
@@ -192,6 +199,7 @@ extern "C" cupf_status cupf_ek2d_create(const cupf_ek2d_params* p, int32_t preci
   h->pitch = (h->fnx + align - 1) / align * align;
   h->plane = (long long)h->pitch * h->fny;
   h->tip_thres = (int)((1.0 - (double)p->blank) * h->fny);
+  h->rows = march_rows(h);
   h->h_rows.assign(h->fny, 0.0);
   auto bail = [&](cupf_status st) {
     cupf_ek2d_destroy(h);

@@ -1,20 +1,21 @@
 // ek2d.cuh — 2D Echebarria–Karma directional-solidification step (psi/U line
 // model of cuPF 2DdendriteMPI/line_model/PF.cu) for sm_100a.
 //
-// One launch advances the whole grid by one step.  A CTA owns a TW x TH tile of
-// output cells and works in four shared-memory phases:
-//   0. load the phase field, U, dpsi of the tile plus a one-cell halo, decode
-//      psi and phi (phi = tanh(psi/sqrt2)) and compute the anti-trapping flux
-//      density jat = (1+(1-k)U)(1-phi^2) dpsi / 2 of every loaded cell;
-//   1. plaquette means of psi and phi at the (i+1/2, j+1/2) corners
-//      (psipjp .. phimjm of merge_PF, PF.cu:444-453);
-//   2. fluxes on every cell edge: the anisotropic psi flux J (atheta/aptheta,
-//      PF.cu:119-146, 475-538) and the solute flux of U with its anti-trapping
-//      part (PF.cu:460-551).  Each edge is computed once and shared by the two
-//      cells it separates (the reference computes it from both sides);
-//   3. per cell: U' = U + dt*div(U flux)/tau_U (PF.cu:553-556), then the psi
-//      right-hand side with the new U (PF.cu:563-590), dpsi = rhs/tau_psi,
-//      psi' = psi + dt*dpsi (+ noise), and the stores.
+// One launch advances the whole grid by one step (ek2d_march_kernel, below):
+// each warp marches up a strip of 30 columns, computing for every cell
+//   - the phase field, U and dpsi of the next row (decoded: psi and
+//     phi = tanh(psi/sqrt2)) and the anti-trapping flux density
+//     jat = (1+(1-k)U)(1-phi^2) dpsi / 2;
+//   - plaquette means of psi and phi at the cell corners (psipjp .. phimjm of
+//     merge_PF, PF.cu:444-453);
+//   - the fluxes through its right and upper edges: the anisotropic psi flux J
+//     (atheta/aptheta, PF.cu:119-146, 475-538) and the solute flux of U with
+//     its anti-trapping part (PF.cu:460-551).  Each edge is computed once and
+//     shared by the two cells it separates (the reference computes it from
+//     both sides);
+//   - U' = U + dt*div(U flux)/tau_U (PF.cu:553-556), then the psi right-hand
+//     side with the new U (PF.cu:563-590), dpsi = rhs/tau_psi,
+//     psi' = psi + dt*dpsi (+ noise), and the stores.
 // The reference's merge_PF (PF.cu:379-610) fuses the same U-then-psi update in
 // one kernel over a 128-wide band of a linear index; the pre-loop rhs_psi
 // (PF.cu:150-280) is the same psi update with U left unchanged (`prestep`).
@@ -24,8 +25,9 @@
 // read; here every writer of an interior cell that some halo cell copies also
 // writes that copy, so each step's output already carries its halo.
 //
-// Storage S: FP32 (the reference's), FP16 / BF16 (split precision: phi (as its
-// distance to the bulk value), U - U0 and dpsi in 16 bits, phi and U stored with
+// Storage S: FP32 (the reference's), FP16 / BF16 (split precision: the phase
+// field (psi bounded to +-50 W0 in FP16; phi as its distance to the bulk value
+// in BF16), U - U0 and dpsi in 16 bits, the phase field and U stored with
 // stochastic rounding, arithmetic in FP32) or FP64 (double arithmetic
 // throughout).  Up = (y/W0 - intR)/lT_tilde of each row
 // is formed in FP64 from the host's FP64 time integration.
@@ -41,10 +43,6 @@
 namespace cupf {
 namespace ek2d {
 
-constexpr int TW = 64;  // output tile width (x, contiguous in memory)
-constexpr int TH = 16;  // output tile height (y)
-constexpr int NTHREADS = 256;
-constexpr int IW = TW + 2, IH = TH + 2;  // input tile with its one-cell halo
 
 // ---- storage formats -------------------------------------------------------
 //
@@ -76,19 +74,25 @@ struct StPlain {
 using StF32 = StPlain<float>;
 using StF64 = StPlain<double>;
 
-// 16-bit storage (split precision) keeps phi, not psi: the phase-field plane
-// holds phi's distance to its nearest bulk value, with phi's sign,
-//   u = copysign(1 - |phi|, phi),   phi = copysign(1 - |u|, u),
-//   |psi| = sqrt2 atanh(1 - |u|) = (ln(2 - |u|) - ln|u|)/sqrt2.
-// A 16-bit float keeps |u| to 11 (FP16) or 8 (BF16) significant bits, i.e. psi
-// to about 3.5e-4 (FP16) or 2.8e-3 (BF16) wherever |psi| >= 1 and about twice
-// that at the interface centre.  psi itself would not do: it is a signed
-// distance that reaches thousands of W0 across the domain, where a 16-bit
-// spacing exceeds the grid's own psi increments, and rounding noise in
-// |grad psi|^2 then drives the far field toward solid.  phi is saturated to
-// +-1 beyond a few W0, so psi is held to |psi| <= kPsiClamp (|u| = 0 there).
+// 16-bit storage (split precision).  psi is a signed distance that reaches
+// thousands of W0 across the domain; stored as it is in 16 bits its spacing
+// there exceeds the grid's own psi increments, and rounding noise in
+// |grad psi|^2 then drives the far field toward solid.  psi is therefore held
+// to |psi| <= kPsiClamp = 50 W0 in the 16-bit modes: far enough that the bound
+// does not reach back to the front (a bound of 12.5 W0, where phi is already
+// +-1 to float precision, moved the front by about a cell in 3000 steps; 25 W0
+// by 0.02 cells; 50 W0 by none measurable), and small enough that FP16 keeps a
+// spacing of at most 0.03 W0 there.
+//   FP16 stores psi itself (spacing 2^-11 |psi|: 5e-4 at the interface centre,
+//   4e-3 at |psi| = 4-8).
+//   BF16, with 8 significant bits, stores phi as its distance to the nearest
+//   bulk value, with phi's sign,
+//     u = copysign(1 - |phi|, phi),   phi = copysign(1 - |u|, u),
+//     |psi| = sqrt2 atanh(1 - |u|) = (ln(2 - |u|) - ln|u|)/sqrt2,
+//   which keeps psi to about 2.8e-3 everywhere (BF16 has FP32's exponent range,
+//   so u of |psi| = 50, 4e-31, is representable).
 // U is stored as its offset from the far-field value U0.
-constexpr float kPsiClamp = 12.5f;
+constexpr float kPsiClamp = 50.0f;
 
 template <bool BF>
 struct StH16 {
@@ -104,18 +108,24 @@ struct StH16 {
   }
   __device__ static V stU(T x, T U0) { return st(__fsub_rn(x, U0)); }
   __device__ static V st_sr(T x, uint32_t r) { return BF ? sr_bf16_bits(x, r) : sr_fp16_bits(x, r); }
-  __device__ static void ld_pp(V v, T, T& ps, T& ph) {
+  __device__ static void ld_pp(V v, T inv_sqrt2, T& ps, T& ph) {
+    if (!BF) {
+      ps = ld(v);
+      ph = tanh_t(ps * inv_sqrt2);
+      return;
+    }
     const float u = ld(v), a = fabsf(u);
     ph = copysignf(1.0f - a, u);
     const float m = (a > 0.0f) ? fminf(0.70710678f * (__logf(2.0f - a) - __logf(a)), kPsiClamp)
                                : kPsiClamp;
     ps = copysignf(m, u);
   }
-  // u of a psi: 1 - tanh(|psi|/sqrt2) = 2/(1 + e^(sqrt2 |psi|)), with psi's sign
+  // the stored value of a psi: psi bounded to +-kPsiClamp (FP16), or its u:
+  // 1 - tanh(|psi|/sqrt2) = 2/(1 + e^(sqrt2 |psi|)) with psi's sign (BF16)
   __device__ static float code(float ps) {
-    const float x = fabsf(ps);
-    const float a = (x >= kPsiClamp) ? 0.0f : __fdividef(2.0f, 1.0f + __expf(1.41421356f * x));
-    return copysignf(a, ps);
+    const float x = fminf(fabsf(ps), kPsiClamp);
+    if (!BF) return copysignf(x, ps);
+    return copysignf(__fdividef(2.0f, 1.0f + __expf(1.41421356f * x)), ps);
   }
   __device__ static V st_ps(T ps) { return st(code(ps)); }
   __device__ static V st_ps_sr(T ps, uint32_t r) { return st_sr(code(ps), r); }
@@ -131,6 +141,7 @@ struct EkArgs {
   long long plane;    // values per plane
   int pitch, fnx, fny;
   int prestep;        // 1: psi update only, U unchanged (rhs_psi)
+  int rows;           // output rows each warp marches over
   float k, hi, Dl_tilde, eps, sqrt2, lamd, dt, cosa, sina, a_s, epsilon, a_12, U0;
   float noise_amp;    // dt_sqrt*hi*eta; 0 disables the noise term
   double up_a, up_b;  // Up of memory row j = up_a + j*up_b
@@ -219,14 +230,6 @@ __device__ __forceinline__ T aniso_a(T phx, T phz, const Consts<T>& c) {
   return (T)1;
 }
 
-template <class T>
-struct Tile {
-  T ps[IH][IW], ph[IH][IW], U[IH][IW], jat[IH][IW];
-  T qs[TH + 1][TW + 1], qp[TH + 1][TW + 1];  // plaquette means of psi, phi
-  T vJ[TH][TW + 1], vU[TH][TW + 1];          // fluxes through x-edges (i+1/2, j)
-  T hJ[TH + 1][TW], hU[TH + 1][TW];          // fluxes through y-edges (i, j+1/2)
-};
-
 // Write one cell's three values at (j, i) and at every halo cell that copies it:
 // column fnx-1 copies column 1 and column 0 copies column fnx-2 (periodic x),
 // row 0 copies row 2 and row fny-1 copies row fny-3 (mirrored y), corners both.
@@ -255,142 +258,202 @@ __device__ __forceinline__ void put_with_halo(V* ps, V* U, V* D, int pitch, int 
   }
 }
 
+// Fluxes through one cell edge, from the differences across it (normal) and
+// along it (tangential, from the plaquette means at its two ends), and the
+// values of the two cells it separates (a below/left, b above/right):
+// J = A (A dpsi_n -+ Ap dpsi_t), the anisotropic psi flux of merge_PF
+// (PF.cu:475-538), and Uf, the solute flux with its anti-trapping part
+// (PF.cu:460-551).  kY selects the y-edge form (normal = z).
+template <bool kY, class T>
+__device__ __forceinline__ void edge_flux(const Consts<T>& c, bool merge, T psx, T psz, T phx,
+                                          T phz, T pha, T phb, T Ua, T Ub, T ja, T jb, T& J,
+                                          T& Uf) {
+  T A, Ap;
+  aniso(phx, phz, c, A, Ap);
+  J = kY ? A * (A * psz + Ap * psx) : A * (A * psx - Ap * psz);
+  if (merge) {
+    const T n2 = phx * phx + phz * phz;
+    const T nn = (n2 > c.eps) ? (kY ? phz : phx) * rsqrt_t(n2) : (T)0;
+    Uf = c.hiDl_half * ((T)2 - pha - phb) * (Ub - Ua) + (T)0.5 * (ja + jb) * nn;
+  }
+}
+
+template <class T>
+__device__ __forceinline__ T jat_of(const Consts<T>& c, T U, T ph, T D) {
+  return (T)0.5 * ((T)1 + c.omk * U) * ((T)1 - ph * ph) * D;
+}
+
+// One cell's update and stores (PF.cu:553-598): U' from the divergence of the
+// solute fluxes, then psi' with the new U, dpsi = rhs/tau_psi, the optional
+// noise term, and the stores with their halo copies.
+template <class S, class T = typename S::T, class V = typename S::V>
+__device__ __forceinline__ void cell_update(const EkArgs& a, const Consts<T>& c, bool merge,
+                                            uint32_t step_key, int gi, int gj, T psC, T phC, T UC,
+                                            T jatC, T JR, T JL, T JT, T JB, T UR, T UL, T UT, T UB,
+                                            T phR, T phL, T phT, T phB, T psR, T psL, T psT,
+                                            T psB, V* o_ps, V* o_U, V* o_D) {
+  T Un = UC;
+  if (merge) {
+    const T rhsU = ((UR - UL) + (UT - UB)) * c.hi + c.sqrt2 * jatC;
+    const T tauU = c.opk - c.omk * phC;
+    Un = UC + c.dt * div_t(rhsU, tauU);
+  }
+  const T phxn = (phR - phL) * (T)0.5;
+  const T phzn = (phT - phB) * (T)0.5;
+  const T psxn = (psR - psL) * (T)0.5;
+  const T pszn = (psT - psB) * (T)0.5;
+  T A2 = aniso_a(phxn, phzn, c);
+  A2 = A2 * A2;
+  const T gradps2 = psxn * psxn + pszn * pszn;
+  const T extra = -c.sqrt2 * A2 * phC * gradps2;
+  const T Up = (T)(a.up_a + (double)gj * a.up_b);
+  const T rhs = ((JR - JL) + (JT - JB) + extra) * c.hi * c.hi + c.sqrt2 * phC -
+                c.lamd * ((T)1 - phC * phC) * c.sqrt2 * (Un + Up);
+  const T tp = (T)1 - c.omk * Up;
+  const T tau = ((tp >= c.k) ? tp : c.k) * A2;
+  const T dps = div_t(rhs, tau);
+  T noise = (T)0;
+  if (c.noise_amp != (T)0 && in_band(phC)) {
+    const Philox4 rn = philox4x32_10((uint32_t)gi, (uint32_t)gj, a.step, 0x4E4F4953u, a.seed, 0x5EEDu);
+    noise = c.noise_amp * ((T)uniform01(rn.v[0]) - (T)0.5);
+  }
+  const T psn = psC + c.dt * dps + noise;
+  V vps, vU, vD;
+  if (S::kSR) {
+    // one 32-bit draw per cell and step: independent 10-bit fractions for the
+    // phase field and U (1/1024 of a 16-bit spacing is ample); dpsi is
+    // rewritten from scratch every step, not accumulated, so it rounds to nearest
+    const uint32_t r = mix32((uint32_t)(gi + a.fnx * gj) ^ step_key);
+    vps = S::st_ps_sr(psn, r & 0xFFC00000u);
+    vU = merge ? S::st_sr(Un - c.U0, (r << 10) & 0xFFC00000u) : S::stU(Un, c.U0);
+    vD = S::st(dps);
+  } else {
+    vps = S::st_ps(psn);
+    vU = S::stU(Un, c.U0);
+    vD = S::st(dps);
+  }
+  put_with_halo(o_ps, o_U, o_D, a.pitch, a.fnx, a.fny, gj, gi, vps, vU, vD);
+}
+
+// ---- register-marching step kernel ------------------------------------------
+//
+// A warp owns a strip of MW = 30 output columns: lane l holds column x0-1+l, so
+// lanes 0 and 31 carry the strip's halo columns.  The warp marches up a.rows
+// output rows, keeping three rows of its own column (r-1, r, r+1) and two of its right
+// neighbour (r, r+1) in registers; the left neighbour's values, plaquette means
+// and x-edge fluxes come by warp shuffle.  Each edge flux is computed once: a
+// lane computes the x-edge on its right and the y-edge above it, the y-edge
+// below it was computed in the previous row.  The next row's loads are issued a
+// row ahead of their use.  No shared memory, no barriers.
+constexpr int MW = 30;
+constexpr int MWARPS = 8;
+
 template <class S>
-__global__ void __launch_bounds__(NTHREADS) ek2d_step_kernel(EkArgs a) {
+__global__ void __launch_bounds__(MWARPS * 32) ek2d_march_kernel(EkArgs a) {
   using T = typename S::T;
   using V = typename S::V;
-  extern __shared__ __align__(16) unsigned char ek_smem[];
-  Tile<T>& sm = *reinterpret_cast<Tile<T>*>(ek_smem);
   const Consts<T> c = consts<T>(a);
   const bool merge = !a.prestep;
   const V* in_ps = static_cast<const V*>(a.in);
   const V* in_U = in_ps + a.plane;
   const V* in_D = in_U + a.plane;
-  const int x0 = 1 + blockIdx.x * TW;  // memory column / row of the first output cell
-  const int y0 = 1 + blockIdx.y * TH;
-
-  // ---- 0. load tile + halo; phi and the anti-trapping density per cell
-  for (int e = threadIdx.x; e < IH * IW; e += NTHREADS) {
-    const int r = e / IW, q = e - r * IW;
-    const int gi = x0 - 1 + q, gj = y0 - 1 + r;
-    T ps = 0, ph = 0, U = 0, D = 0;
-    if (gi < a.fnx && gj < a.fny) {
-      const long long o = (long long)gj * a.pitch + gi;
-      S::ld_pp(in_ps[o], c.inv_sqrt2, ps, ph);
-      U = S::ldU(in_U[o], c.U0);
-      D = S::ld(in_D[o]);
-    }
-    sm.ps[r][q] = ps;
-    sm.ph[r][q] = ph;
-    sm.U[r][q] = U;
-    sm.jat[r][q] = (T)0.5 * ((T)1 + c.omk * U) * ((T)1 - ph * ph) * D;
-  }
-  __syncthreads();
-
-  // ---- 1. plaquette means (corner (q+1/2, r+1/2) of the input tile)
-  for (int e = threadIdx.x; e < (TH + 1) * (TW + 1); e += NTHREADS) {
-    const int r = e / (TW + 1), q = e - r * (TW + 1);
-    sm.qs[r][q] = (((sm.ps[r][q] + sm.ps[r][q + 1]) + sm.ps[r + 1][q]) + sm.ps[r + 1][q + 1]) * (T)0.25;
-    sm.qp[r][q] = (((sm.ph[r][q] + sm.ph[r][q + 1]) + sm.ph[r + 1][q]) + sm.ph[r + 1][q + 1]) * (T)0.25;
-  }
-  __syncthreads();
-
-  // ---- 2. edge fluxes
-  constexpr int NV = TH * (TW + 1), NHZ = (TH + 1) * TW;
-  for (int e = threadIdx.x; e < NV + NHZ; e += NTHREADS) {
-    if (e < NV) {
-      // x-edge between input cells (b+1, q) and (b+1, q+1)
-      const int b = e / (TW + 1), q = e - b * (TW + 1);
-      const T psx = sm.ps[b + 1][q + 1] - sm.ps[b + 1][q];
-      const T psz = sm.qs[b + 1][q] - sm.qs[b][q];
-      const T phx = sm.ph[b + 1][q + 1] - sm.ph[b + 1][q];
-      const T phz = sm.qp[b + 1][q] - sm.qp[b][q];
-      T A, Ap;
-      aniso(phx, phz, c, A, Ap);
-      sm.vJ[b][q] = A * (A * psx - Ap * psz);
-      if (merge) {
-        const T n2 = phx * phx + phz * phz;
-        const T nx = (n2 > c.eps) ? phx * rsqrt_t(n2) : (T)0;
-        sm.vU[b][q] = c.hiDl_half * ((T)2 - sm.ph[b + 1][q] - sm.ph[b + 1][q + 1]) *
-                          (sm.U[b + 1][q + 1] - sm.U[b + 1][q]) +
-                      (T)0.5 * (sm.jat[b + 1][q] + sm.jat[b + 1][q + 1]) * nx;
-      }
-    } else {
-      // y-edge between input cells (r, q+1) and (r+1, q+1)
-      const int f = e - NV;
-      const int r = f / TW, q = f - r * TW;
-      const T psz = sm.ps[r + 1][q + 1] - sm.ps[r][q + 1];
-      const T psx = sm.qs[r][q + 1] - sm.qs[r][q];
-      const T phz = sm.ph[r + 1][q + 1] - sm.ph[r][q + 1];
-      const T phx = sm.qp[r][q + 1] - sm.qp[r][q];
-      T A, Ap;
-      aniso(phx, phz, c, A, Ap);
-      sm.hJ[r][q] = A * (A * psz + Ap * psx);
-      if (merge) {
-        const T n2 = phx * phx + phz * phz;
-        const T nz = (n2 > c.eps) ? phz * rsqrt_t(n2) : (T)0;
-        sm.hU[r][q] = c.hiDl_half * ((T)2 - sm.ph[r][q + 1] - sm.ph[r + 1][q + 1]) *
-                          (sm.U[r + 1][q + 1] - sm.U[r][q + 1]) +
-                      (T)0.5 * (sm.jat[r][q + 1] + sm.jat[r + 1][q + 1]) * nz;
-      }
-    }
-  }
-  __syncthreads();
-
-  // ---- 3. cell updates
   V* o_ps = static_cast<V*>(a.out);
   V* o_U = o_ps + a.plane;
   V* o_D = o_U + a.plane;
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int x0 = 1 + (blockIdx.x * MWARPS + warp) * MW;  // first output column of the strip
+  if (x0 > a.fnx - 2) return;                              // whole warp: uniform
+  const int gi = x0 - 1 + lane;
+  const bool col_ok = gi < a.fnx;
+  const bool out_col = lane >= 1 && lane <= MW && gi <= a.fnx - 2;
+  const int y0 = 1 + blockIdx.y * a.rows;
   const uint32_t step_key = mix32(a.step ^ (a.seed * 0x9E3779B9u));
-  for (int e = threadIdx.x; e < TH * TW; e += NTHREADS) {
-    const int b = e / TW, q = e - b * TW;
-    const int gi = x0 + q, gj = y0 + b;
-    if (gi > a.fnx - 2 || gj > a.fny - 2) continue;
-    const int r = b + 1, s = q + 1;  // input-tile coordinates of the cell
-    const T psC = sm.ps[r][s], phC = sm.ph[r][s], UC = sm.U[r][s];
-    T Un = UC;
-    if (merge) {
-      const T rhsU = ((sm.vU[b][q + 1] - sm.vU[b][q]) + (sm.hU[b + 1][q] - sm.hU[b][q])) * c.hi +
-                     c.sqrt2 * sm.jat[r][s];
-      const T tauU = c.opk - c.omk * phC;
-      Un = UC + c.dt * div_t(rhsU, tauU);
+
+  // raw values of the next row to decode, loaded one row ahead of their use so
+  // that the load latency overlaps the current row's arithmetic
+  V raw_ps{}, raw_U{}, raw_D{};
+  bool raw_ok = false;
+  auto issue = [&](int r) {
+    raw_ok = col_ok && r < a.fny;
+    if (raw_ok) {
+      const long long o = (long long)r * a.pitch + gi;
+      raw_ps = in_ps[o];
+      raw_U = in_U[o];
+      raw_D = in_D[o];
     }
-    const T phxn = (sm.ph[r][s + 1] - sm.ph[r][s - 1]) * (T)0.5;
-    const T phzn = (sm.ph[r + 1][s] - sm.ph[r - 1][s]) * (T)0.5;
-    const T psxn = (sm.ps[r][s + 1] - sm.ps[r][s - 1]) * (T)0.5;
-    const T pszn = (sm.ps[r + 1][s] - sm.ps[r - 1][s]) * (T)0.5;
-    T A2 = aniso_a(phxn, phzn, c);
-    A2 = A2 * A2;
-    const T gradps2 = psxn * psxn + pszn * pszn;
-    const T extra = -c.sqrt2 * A2 * phC * gradps2;
-    const T Up = (T)(a.up_a + (double)gj * a.up_b);
-    const T rhs = ((sm.vJ[b][q + 1] - sm.vJ[b][q]) + (sm.hJ[b + 1][q] - sm.hJ[b][q]) + extra) * c.hi *
-                      c.hi +
-                  c.sqrt2 * phC - c.lamd * ((T)1 - phC * phC) * c.sqrt2 * (Un + Up);
-    const T tp = (T)1 - c.omk * Up;
-    const T tau = ((tp >= c.k) ? tp : c.k) * A2;
-    const T dps = div_t(rhs, tau);
-    T noise = (T)0;
-    if (c.noise_amp != (T)0 && in_band(phC)) {
-      const Philox4 rn = philox4x32_10((uint32_t)gi, (uint32_t)gj, a.step, 0x4E4F4953u, a.seed, 0x5EEDu);
-      noise = c.noise_amp * ((T)uniform01(rn.v[0]) - (T)0.5);
+  };
+  auto load = [&](T& ps, T& ph, T& U, T& jat) {
+    ps = ph = U = jat = (T)0;
+    if (raw_ok) {
+      S::ld_pp(raw_ps, c.inv_sqrt2, ps, ph);
+      U = S::ldU(raw_U, c.U0);
+      jat = jat_of(c, U, ph, S::ld(raw_D));
     }
-    const T psn = psC + c.dt * dps + noise;
-    V vps, vU, vD;
-    if (S::kSR) {
-      // one 32-bit draw per cell and step: independent 10-bit fractions for psi
-      // and U (1/1024 of a 16-bit spacing is ample); dpsi is rewritten from
-      // scratch every step, not accumulated, so it rounds to nearest
-      const uint32_t r = mix32((uint32_t)(gi + a.fnx * gj) ^ step_key);
-      vps = S::st_ps_sr(psn, r & 0xFFC00000u);
-      vU = merge ? S::st_sr(Un - c.U0, (r << 10) & 0xFFC00000u) : S::stU(Un, c.U0);
-      vD = S::st(dps);
-    } else {
-      vps = S::st_ps(psn);
-      vU = S::stU(Un, c.U0);
-      vD = S::st(dps);
-    }
-    put_with_halo(o_ps, o_U, o_D, a.pitch, a.fnx, a.fny, gj, gi, vps, vU, vD);
+  };
+  auto right = [&](T v) { return __shfl_down_sync(FULL, v, 1); };
+  auto left = [&](T v) { return __shfl_up_sync(FULL, v, 1); };
+
+  // row r+1 ("c") and its right neighbour; row r ("b"); row r-1 ("a")
+  T ps_c, ph_c, U_c, j_c, Rps_c, Rph_c, RU_c, Rj_c;
+  T ps_b, ph_b, U_b, j_b, Rps_b, Rph_b, RU_b, Rj_b;
+  T ps_a, ph_a;
+  auto fetch_c = [&]() {  // decode the issued row into "c"
+    load(ps_c, ph_c, U_c, j_c);
+    Rps_c = right(ps_c);
+    Rph_c = right(ph_c);
+    RU_c = right(U_c);
+    Rj_c = right(j_c);
+  };
+  auto shift = [&]() {
+    ps_a = ps_b;
+    ph_a = ph_b;
+    ps_b = ps_c; ph_b = ph_c; U_b = U_c; j_b = j_c;
+    Rps_b = Rps_c; Rph_b = Rph_c; RU_b = RU_c; Rj_b = Rj_c;
+  };
+  // plaquette means at (x+1/2, r+1/2) from rows b and c
+  auto plaq = [&](T& qs, T& qp) {
+    qs = (((ps_b + Rps_b) + ps_c) + Rps_c) * (T)0.25;
+    qp = (((ph_b + Rph_b) + ph_c) + Rph_c) * (T)0.25;
+  };
+  // y-edge (x, r+1/2) between rows b and c
+  auto yedge = [&](T qs, T qp, T& J, T& Uf) {
+    const T Lqs = left(qs), Lqp = left(qp);
+    edge_flux<true>(c, merge, qs - Lqs, ps_c - ps_b, qp - Lqp, ph_c - ph_b, ph_b, ph_c, U_b, U_c,
+                    j_b, j_c, J, Uf);
+  };
+
+  issue(y0 - 1);
+  fetch_c();
+  shift();
+  issue(y0);
+  fetch_c();
+  issue(y0 + 1);
+  T qs_hi, qp_hi;
+  plaq(qs_hi, qp_hi);
+  T yJ_hi, yU_hi = (T)0;
+  yedge(qs_hi, qp_hi, yJ_hi, yU_hi);
+
+  for (int t = 0; t < a.rows; ++t) {
+    const int r = y0 + t;
+    if (r > a.fny - 2) break;  // uniform across the warp
+    shift();
+    fetch_c();      // row r+1, issued one row earlier
+    issue(r + 2);   // in flight during this row's arithmetic
+    const T qs_lo = qs_hi, qp_lo = qp_hi;
+    plaq(qs_hi, qp_hi);
+    // x-edge (x+1/2, r)
+    T xJ, xU = (T)0;
+    edge_flux<false>(c, merge, Rps_b - ps_b, qs_hi - qs_lo, Rph_b - ph_b, qp_hi - qp_lo, ph_b, Rph_b,
+                     U_b, RU_b, j_b, Rj_b, xJ, xU);
+    const T yJ_lo = yJ_hi, yU_lo = yU_hi;
+    yedge(qs_hi, qp_hi, yJ_hi, yU_hi);
+    const T xJ_L = left(xJ), xU_L = left(xU);
+    const T Lps = left(ps_b), Lph = left(ph_b);
+    if (out_col)
+      cell_update<S>(a, c, merge, step_key, gi, r, ps_b, ph_b, U_b, j_b, xJ, xJ_L, yJ_hi, yJ_lo, xU,
+                     xU_L, yU_hi, yU_lo, Rph_b, Lph, ph_c, ph_a, Rps_b, Lps, ps_c, ps_a, o_ps, o_U,
+                     o_D);
   }
 }
 

@@ -24,10 +24,11 @@
  * split-precision error at sizes the CPU oracle cannot run) store psi and
  * recompute phi = tanh(psi/sqrt2) wherever it is read, as the reference's
  * merge_PF stores it right after computing psi (PF.cu:596).  FP16 and BF16
- * (split precision, all arithmetic FP32) store phi as its distance to the
- * nearest bulk value (psi = sqrt2 atanh(phi) is recovered from it and held to
- * |psi| <= 12.5, where phi is +-1 to float precision), U as its offset from
- * U0, and dpsi; phi and U are stored with stochastic rounding.  Time, the integrated pulling distance, the frame's y
+ * (split precision, all arithmetic FP32) hold psi to |psi| <= 50 W0 (a signed
+ * distance, it would otherwise reach thousands of W0, beyond what 16 bits
+ * resolve) and store it as psi (FP16) or as phi's distance to the nearest bulk
+ * value (BF16), U as its offset from U0, and dpsi; the phase field and U are
+ * stored with stochastic rounding.  Time, the integrated pulling distance, the frame's y
  * coordinates and the row sums of the tip search are FP64 for every storage.
  */
 #ifndef CUPF_EK2D_H_

@@ -124,7 +124,9 @@ def test_fp64_device_matches_fp64_oracle(built):
     assert info["shifts"] == s["info"].shifts > 0
     rec = {k: float(np.abs(_interior(d[k]) - _interior(s[k])).max()) for k in ("psi", "phi", "U", "dpsi")}
     _record("ek2d_fp64_vs_oracle.json", rec)
-    assert rec["phi"] < 1e-9 and rec["U"] < 1e-9, rec
+    # both in double; they differ in operand order (shared edge fluxes), and the
+    # growing front amplifies those 1e-16 differences over 300 steps
+    assert rec["phi"] < 1e-7 and rec["U"] < 1e-7, rec
     assert rec["psi"] < 1e-8 * np.abs(s["psi"]).max(), rec
 
 
@@ -168,6 +170,9 @@ def test_split_precision_error_2d(built, split_reference, prec):
     assert adv > 0.5 * dxd, rec  # the front moved
     if prec in ("fp32", "fp64"):
         assert rec["tip_advance_rel_err"] < 1e-3, rec
+    else:
+        # 16-bit storage: the tip within a quarter of a cell of FP64 after 3000 steps
+        assert rec["tip_position_err_cells"] < 0.25, rec
 
 
 def test_phase_field_2d_executable(built, tmp_path):
