@@ -152,7 +152,7 @@ def directional_case(nx, ny, steps, G=0.1, R=1.0e4, front_frac=0.3, sites=32, am
     lD = float(p.Dl) / float(R)
     yy = y_mac.astype(np.float64)
     psi_mac = (-yy / W0).astype(np.float32)
-    U_mac = np.where(yy > 0, -1.0 + np.exp(-yy / lD), 0.0).astype(np.float32)
+    U_mac = np.where(yy > 0, -1.0 + np.exp(-np.maximum(yy, 0.0) / lD), 0.0).astype(np.float32)
     p.y0 = float(y_mac[0])
     x, y, psi, phi, U = initial_fields(p, y_mac, psi_mac, U_mac)
     perturb(p, psi, phi, sites, amp)
