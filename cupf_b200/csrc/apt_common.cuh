@@ -42,6 +42,7 @@ struct StepArgs {
   const float* z;
   const float* sint;
   const float* cost;
+  const float4* orient;  // per orientation index 0..NG: {sint[i], cost[i], sint[i+NG], cost[i+NG]}
   const float* X_mac;
   const float* Y_mac;
   const float* Z_mac;
@@ -61,5 +62,17 @@ __host__ __device__ __forceinline__ int bc_map(int c, int fn, int bc) {
 }
 
 enum ErrCode { ERR_TMA_TIMEOUT = 1 };
+
+// Orientation table of the step: entry i (0..num_theta) packs the two angles'
+// sines and cosines {sint[i], cost[i], sint[i+NG], cost[i+NG]} so that a slot
+// update reads them with one 16-byte load.  sint/cost have 2*NG+1 entries.
+inline void pack_orientations(const float* sint, const float* cost, int num_theta, float* out) {
+  for (int i = 0; i <= num_theta; ++i) {
+    out[4 * i + 0] = sint[i];
+    out[4 * i + 1] = cost[i];
+    out[4 * i + 2] = sint[i + num_theta];
+    out[4 * i + 3] = cost[i + num_theta];
+  }
+}
 
 }  // namespace cupf

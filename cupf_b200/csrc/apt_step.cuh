@@ -53,6 +53,17 @@ struct StepSmem {
 template <int NP>
 using CodeMap = typename std::conditional<(NP <= 8), uint32_t, unsigned long long>::type;
 
+// Replace 4-bit field j of a code map with v (one bfi for 32-bit maps).
+__device__ __forceinline__ uint32_t nib_insert(uint32_t c, uint32_t v, int j) {
+  uint32_t r;
+  asm("bfi.b32 %0, %1, %2, %3, 4;" : "=r"(r) : "r"(v), "r"(c), "r"(4 * j));
+  return r;
+}
+__device__ __forceinline__ unsigned long long nib_insert(unsigned long long c, uint32_t v, int j) {
+  const int sh = 4 * j;
+  return (c & ~(0xFull << sh)) | ((unsigned long long)v << sh);
+}
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
@@ -152,6 +163,7 @@ template <int NP, class S>
 __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArgs& a, int txi,
                                           int tyi, int zci, CtaSmem<NP, S>& sm, int& qbase) {
   using Map = CodeMap<NP>;
+  static_assert(NP <= 8, "slot codes are 4-bit fields of one 32-bit word");
   using Smem = StepSmem<NP, S>;
   using P = typename S::T;
   constexpr int BW = Smem::BW;
@@ -290,8 +302,9 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
       code[s] = ~(Map)0;
       alias[s] = -1.0f;
     }
-#pragma unroll
-    for (int s = 0; s < 7; ++s) {
+    // General visit of stencil point s: each occupied slot's id is looked up in
+    // the list and appended when new (APTPhaseField.cu:211-233).
+    auto merge_point = [&](int s) {
       uint32_t m = mk[s];
       while (m) {
         const int p = __ffs(m) - 1;
@@ -311,21 +324,67 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
           } else {
             // local_phs[s][NUM_PF] aliases local_phs[s+1][0]; past the array at s == 6
             if (s < 6) {
-              code[s + 1] = (code[s + 1] & ~(Map)0xF) | (Map)0xE;
+              code[s + 1] = nib_insert(code[s + 1], 0xEu, 0);
               alias[s + 1] = S::phi(pr);
             }
             continue;
           }
         }
-        const int sh = 4 * j;
-        code[s] = (code[s] & ~((Map)0xF << sh)) | ((Map)p << sh);
+        code[s] = nib_insert(code[s], (uint32_t)p, j);
+      }
+    };
+    // A point whose every occupied slot q holds the id already at list position
+    // q maps q to q and adds nothing to the list: the general visit finds each of
+    // its ids at q (the list holds distinct ids).  The centre and the point above
+    // nearly always satisfy this, because every cell's slot order is the
+    // first-seen order of its own neighbourhood, which starts with the column.
+    auto identity_point = [&](int s) -> bool {
+      const uint32_t m = mk[s];
+      bool ok = true;
+      Map occ = 0;
+#pragma unroll
+      for (int q = 0; q < NP; ++q)
+        if ((m >> q) & 1u) {
+          ok = ok && (S::id(pts[s][q * BCELLS]) == L[q]);
+          occ |= (Map)0xF << (4 * q);
+        }
+      if (ok) code[s] = (code[s] & ~occ) | ((Map)0x76543210u & occ);
+      return ok;
+    };
+    // The point below comes first: the list is empty, so its slot p can only meet
+    // the ids of its own lower slots (n <= p, and the list cannot overflow).
+    {
+      const uint32_t m = mk[0];
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        if (!((m >> p) & 1u)) continue;
+        const int id = S::id(pts[0][p * BCELLS]);
+        int j = n;
+#pragma unroll
+        for (int q = p - 1; q >= 0; --q)
+          if (L[q] == id) j = q;
+        if (j == n) {
+#pragma unroll
+          for (int q = 0; q <= p; ++q)
+            if (q == n) L[q] = id;
+          ++n;
+        }
+        code[0] = nib_insert(code[0], (uint32_t)p, j);
       }
     }
+    merge_point(1);
+    merge_point(2);
+    if (!identity_point(3)) merge_point(3);
+    merge_point(4);
+    merge_point(5);
+    if (!identity_point(6)) merge_point(6);
 
+    // Value of output slot j at stencil point s: 0xF = absent (-1), 0xE = the
+    // aliased overflow value, which only ever lands in slot 0.
     auto fetch = [&](int s, int j) -> float {
       const uint32_t cd = (uint32_t)(code[s] >> (4 * j)) & 0xF;
+      if (j == 0 && cd == 0xE) return alias[s];
       if (cd == 0xF) return -1.0f;
-      if (cd == 0xE) return alias[s];
       return S::phi(pts[s][cd * BCELLS]);
     };
 
@@ -371,17 +430,16 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
         if (id > a.num_theta) tid2 = (id % a.num_theta) + 1;
         const bool tab_ok = (unsigned)tid2 <= (unsigned)a.num_theta;
         const int ti = tab_ok ? tid2 : 0;
-        const float t_sa = __ldg(a.sint + ti), t_ca = __ldg(a.cost + ti);
-        const float t_sb = __ldg(a.sint + ti + a.num_theta), t_cb = __ldg(a.cost + ti + a.num_theta);
+        const float4 t_o = __ldg(a.orient + ti);  // {sint[ti], cost[ti], sint[ti+NG], cost[ti+NG]}
         float ph7[7];
 #pragma unroll
         for (int s = 0; s < 7; ++s) ph7[s] = fetch(s, j);
         float sina = 0.0f, cosa = 1.0f, sinb = 0.0f, cosb = 1.0f;
         if (ph7[3] > kLS && tab_ok) {  // (double)phC > LS
-          sina = t_sa;
-          cosa = t_ca;
-          sinb = t_sb;
-          cosb = t_cb;
+          sina = t_o.x;
+          cosa = t_o.y;
+          sinb = t_o.z;
+          cosb = t_o.w;
         }
         float repul = 0.0f;
 #pragma unroll

@@ -50,16 +50,41 @@ __device__ __forceinline__ KineConst kine_const(float kd) {
   return k;
 }
 
-// 4-fold kinetic anisotropy of the rotated normal (APTPhaseField.cu:36-52).
+// Normal rotated into the grain frame.  APT kernel (APTPhaseField.cu:41-46):
+//   ( ca*cb*ux + sa*cb*uy - sb*uz,  -sa*ux + ca*uy + 0,  ca*sb*ux + sa*sb*uy + cb*uz );
+// full-PF kernel (kFull, PhaseField.cu:37-44), a different rotation:
+//   ( ca*cb*ux + sa*uy + ca*sb*uz,  -sa*cb*ux + ca*uy - sa*sb*uz,  -sb*ux + 0 + cb*uz ).
+// The full-PF sums take the fusions of the APT sums of the same shape.
+template <bool kFull>
+__device__ __forceinline__ void rotate_normal(float ux, float uy, float uz, float cosa, float sina,
+                                              float cosb, float sinb, float& rx, float& ry,
+                                              float& rz) {
+  using K = Contract;
+  if (!kFull) {
+    float s = sop<K::UX_IN>(fmul(cosa, cosb), ux, fmul(sina, cosb), uy);
+    rx = K::UX_OUT ? ffma(-sinb, uz, s) : fsub(s, fmul(sinb, uz));
+    ry = fadd(sop<K::UY>(-sina, ux, cosa, uy), 0.0f);
+    s = sop<K::UZ_IN>(fmul(cosa, sinb), ux, fmul(sina, sinb), uy);
+    rz = K::UZ_OUT ? ffma(cosb, uz, s) : fadd(s, fmul(cosb, uz));
+  } else {
+    float s = sop<K::UX_IN>(fmul(cosa, cosb), ux, sina, uy);
+    rx = K::UX_OUT ? ffma(fmul(cosa, sinb), uz, s) : fadd(s, fmul(fmul(cosa, sinb), uz));
+    s = sop<K::UX_IN>(fmul(-sina, cosb), ux, cosa, uy);
+    ry = K::UX_OUT ? ffma(-fmul(sina, sinb), uz, s) : fsub(s, fmul(fmul(sina, sinb), uz));
+    s = fadd(fmul(-sinb, ux), 0.0f);
+    rz = K::UZ_OUT ? ffma(cosb, uz, s) : fadd(s, fmul(cosb, uz));
+  }
+}
+
+// 4-fold kinetic anisotropy of the rotated normal (APTPhaseField.cu:36-52,
+// PhaseField.cu:32-50).
+template <bool kFull = false>
 __device__ __forceinline__ float kine_ani(float ux, float uy, float uz, float cosa, float sina,
                                           float cosb, float sinb, KineConst kc, float eps) {
   using K = Contract;
   const float a_s = kc.a_s, epsilon = kc.epsilon;
-  float s = sop<K::UX_IN>(fmul(cosa, cosb), ux, fmul(sina, cosb), uy);
-  float rx = K::UX_OUT ? ffma(-sinb, uz, s) : fsub(s, fmul(sinb, uz));
-  float ry = fadd(sop<K::UY>(-sina, ux, cosa, uy), 0.0f);
-  s = sop<K::UZ_IN>(fmul(cosa, sinb), ux, fmul(sina, sinb), uy);
-  float rz = K::UZ_OUT ? ffma(cosb, uz, s) : fadd(s, fmul(cosb, uz));
+  float rx, ry, rz;
+  rotate_normal<kFull>(ux, uy, uz, cosa, sina, cosb, sinb, rx, ry, rz);
   float ux2 = fmul(rx, rx), uy2 = fmul(ry, ry), uz2 = fmul(rz, rz);
   float mag = sop<K::MAG_IN>(rx, rx, ry, ry);
   mag = K::MAG_OUT ? ffma(rz, rz, mag) : fadd(mag, uz2);
@@ -144,9 +169,12 @@ __device__ __forceinline__ bool tinterp(const StepArgs& a, int i, int j, int k, 
   return true;
 }
 
-// New phi of one active slot (APTPhaseField.cu:254-340).  ph[0..6] are the
-// slot's values at D,B,L,C,R,T,U; repul the repulsion sum; Up = T/L_cp.
-__device__ __forceinline__ float slot_update(const StepArgs& a, KineConst kc, const float ph[7],
+// New phi of one active slot (APTPhaseField.cu:254-340; the full-PF kernel's
+// PhaseField.cu:195-297 is the same arithmetic with its own rotation, kFull).
+// ph[0..6] are the slot's values at D,B,L,C,R,T,U; repul the repulsion sum;
+// Up = T/L_cp.  A: launch arguments with eps, hi, lamd and dt.
+template <bool kFull = false, class A>
+__device__ __forceinline__ float slot_update(const A& a, KineConst kc, const float ph[7],
                                              float sina, float cosa, float sinb, float cosb,
                                              float repul, float Up) {
   using K = Contract;
@@ -155,7 +183,7 @@ __device__ __forceinline__ float slot_update(const StepArgs& a, KineConst kc, co
   float phx = fmul(fsub(phR, phL), 0.5f);
   float phy = fmul(fsub(phT, phB), 0.5f);
   float phz = fmul(fsub(phU, phD), 0.5f);
-  float A2 = kine_ani(phx, phy, phz, cosa, sina, cosb, sinb, kc, a.eps);
+  float A2 = kine_ani<kFull>(phx, phy, phz, cosa, sina, cosb, sinb, kc, a.eps);
   float sum = fadd(fadd(fadd(fadd(fadd(phR, phL), phT), phB), phU), phD);
   float diff = K::DIFF ? ffma(-6.0f, phC, sum) : fsub(sum, fmul(6.0f, phC));
   float w = K::W ? ffma(-phC, phC, 1.0f) : fsub(1.0f, fmul(phC, phC));

@@ -80,6 +80,7 @@ struct cupf_apt_handle {
   cudaStream_t stream = nullptr;
   // device inputs
   float *x = nullptr, *y = nullptr, *z = nullptr, *sint = nullptr, *cost = nullptr;
+  float* orient = nullptr;  // packed orientation table (pack_orientations)
   float *X_mac = nullptr, *Y_mac = nullptr, *Z_mac = nullptr, *t_mac = nullptr;
   float *psi_mac = nullptr, *T_3D = nullptr;
   bool has_T3D = false;
@@ -183,7 +184,7 @@ static cupf_status make_tmap(cupf_apt_handle* h, int b) {
 static void free_handle(cupf_apt_handle* h) {
   if (!h) return;
   cudaSetDevice(h->device);
-  void* ptrs[] = {h->buf[0], h->buf[1], h->x, h->y, h->z, h->sint, h->cost, h->X_mac, h->Y_mac,
+  void* ptrs[] = {h->buf[0], h->buf[1], h->x, h->y, h->z, h->sint, h->cost, h->orient, h->X_mac, h->Y_mac,
                   h->Z_mac, h->t_mac, h->psi_mac, h->T_3D, h->phi_m, h->alpha_m, h->err, h->work,
                   h->xfer_ph, h->xfer_id, h->layer_sums, h->alpha_full, h->loss_area,
                   h->counts, h->first, h->qoi_part, h->nucl_status, h->nucl_count,
@@ -281,6 +282,7 @@ static StepArgs step_args(cupf_apt_handle* h, float t, int use_iuc) {
   a.z = h->z;
   a.sint = h->sint;
   a.cost = h->cost;
+  a.orient = reinterpret_cast<const float4*>(h->orient);
   a.X_mac = h->X_mac;
   a.Y_mac = h->Y_mac;
   a.Z_mac = h->Z_mac;
@@ -393,6 +395,11 @@ extern "C" cupf_status cupf_apt_create(const cupf_apt_params* p, const cupf_apt_
   h->z_host.assign(in->z, in->z + p->fnz);
   TRY(upload(&h->sint, in->sint, nth, h->stream));
   TRY(upload(&h->cost, in->cost, nth, h->stream));
+  {
+    std::vector<float> ot(4 * (size_t)(p->num_theta + 1));
+    pack_orientations(in->sint, in->cost, p->num_theta, ot.data());
+    TRY(upload(&h->orient, ot.data(), ot.size(), h->stream));
+  }
   const size_t mNx = p->Nx > 0 ? p->Nx : 1, mNy = p->Ny > 0 ? p->Ny : 1;
   const size_t mNz = p->Nz > 0 ? p->Nz : 1, mNt = p->Nt > 0 ? p->Nt : 1;
   TRY(upload(&h->X_mac, in->X_mac, in->X_mac ? mNx : 2, h->stream));

@@ -63,7 +63,7 @@ enum ReqState { PENDING = 0, RUNNING = 1, DONE = 2, FAILED = 3 };
 struct Request {
   int64_t id = 0;
   cupf_apt_params p;
-  std::vector<float> x, y, z, sint, cost, phi;
+  std::vector<float> x, y, z, sint, cost, orient, phi;
   std::vector<int> alpha;
   int64_t nsteps = 0;
   int state = PENDING;
@@ -73,6 +73,7 @@ struct Request {
   Grid g;
   void* buf[2] = {nullptr, nullptr};
   float *dx = nullptr, *dy = nullptr, *dz = nullptr, *dsint = nullptr, *dcost = nullptr;
+  float* dorient = nullptr;
   float* dphi = nullptr;
   int* dalpha = nullptr;
   float* ddummy = nullptr;
@@ -130,12 +131,12 @@ static int gridn(long long n) {
 }
 
 static void free_request_device(Request* r) {
-  void* ptrs[] = {r->buf[0], r->buf[1], r->dx, r->dy, r->dz, r->dsint, r->dcost, r->dphi,
+  void* ptrs[] = {r->buf[0], r->buf[1], r->dx, r->dy, r->dz, r->dsint, r->dcost, r->dorient, r->dphi,
                   r->dalpha, r->ddummy};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   r->buf[0] = r->buf[1] = nullptr;
-  r->dx = r->dy = r->dz = r->dsint = r->dcost = r->dphi = nullptr;
+  r->dx = r->dy = r->dz = r->dsint = r->dcost = r->dorient = r->dphi = nullptr;
   r->dalpha = nullptr;
   r->ddummy = nullptr;
 }
@@ -215,7 +216,8 @@ static cupf_status admit(cupf_server* s, Request* r, int slot) {
   for (int b = 0; b < 2; ++b) CK(cudaMalloc(&r->buf[b], bb));
   cupf_status e;
   if ((e = up(&r->dx, r->x)) || (e = up(&r->dy, r->y)) || (e = up(&r->dz, r->z)) ||
-      (e = up(&r->dsint, r->sint)) || (e = up(&r->dcost, r->cost)) || (e = up(&r->dphi, r->phi)))
+      (e = up(&r->dsint, r->sint)) || (e = up(&r->dcost, r->cost)) ||
+      (e = up(&r->dorient, r->orient)) || (e = up(&r->dphi, r->phi)))
     return e;
   (void)nth;
   CK(cudaMalloc((void**)&r->dalpha, L * sizeof(int)));
@@ -295,6 +297,7 @@ static cupf_status admit(cupf_server* s, Request* r, int slot) {
   a.z = r->dz;
   a.sint = r->dsint;
   a.cost = r->dcost;
+  a.orient = reinterpret_cast<const float4*>(r->dorient);
   a.X_mac = r->ddummy;
   a.Y_mac = r->ddummy;
   a.Z_mac = r->ddummy;
@@ -527,6 +530,8 @@ extern "C" cupf_status cupf_server_submit(cupf_server* s, const cupf_apt_params*
   const int nth = 2 * p->num_theta + 1;
   r->sint.assign(in->sint, in->sint + nth);
   r->cost.assign(in->cost, in->cost + nth);
+  r->orient.resize(4 * (size_t)(p->num_theta + 1));
+  pack_orientations(in->sint, in->cost, p->num_theta, r->orient.data());
   const size_t L = (size_t)p->fnx * p->fny * p->fnz;
   r->phi.assign(phi, phi + L);
   r->alpha.assign(alpha, alpha + L);
