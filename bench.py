@@ -367,6 +367,119 @@ def run_ek2d(args):
     return 0
 
 
+DENSE_INTERIOR = (128, 128, 128)
+DENSE_GRAINS = 80   # the line case's grain density of 600 grains on 256x256
+
+
+def dense_cpu_baseline(case, budget_s=15.0):
+    """The full-PF oracle (FP32, OpenMP over all host threads) on the same case."""
+    from oracle import DenseOracle
+    o = DenseOracle()
+    p = case.params
+    ph = o.ini(p, case.phi, case.alpha)
+    steps, t_total = 0, 0.0
+    a = ph
+    while t_total < budget_s and steps < 40:
+        t0 = time.perf_counter()
+        a, _ = o.run(case, case.meta["R"], a, 2, step0=steps)
+        t_total += time.perf_counter() - t0
+        steps += 2
+    cells = (p.fnx - 2) * (p.fny - 2) * (p.fnz - 2)
+    return {"value": cells * steps / t_total / 1e6, "unit": "Mcell-upd/s", "cores": os.cpu_count(),
+            "kind": "port", "sample": "%d full-PF oracle steps of the same case from the initial "
+                                      "state (%.1f s)" % (steps, t_total)}
+
+
+def run_dense(args):
+    """The full (non-APT, -a) mode: one phi field per grain.  The library's
+    two-launch step, the reference's own set_BC_3D + rhs_psi pair on the same
+    state, and the APT step on the same case (the speed-up the -a comparison is
+    for), each timed on the device after warm-up steps from the initial state."""
+    import ctypes as C
+    import torch
+    from cupf_b200 import cases
+    from cupf_b200.dense import DenseSolver
+    from cupf_b200.solver import APTSolver
+    nx, ny, nz = DENSE_INTERIOR if not args.interior else tuple(args.interior)
+    ng = max(4, int(DENSE_GRAINS * nx * ny / (DENSE_INTERIOR[0] * DENSE_INTERIOR[1])))
+    case = cases.line_case(nx, ny, nz, num_pf=NUM_PF, num_grains=ng, seed=SEED, bc="110")
+    p = case.params
+    cells = nx * ny * nz
+    R = case.meta["R"]
+    steps, warm = args.steps, max(args.warmup, 3)
+    with DenseSolver(case) as s:
+        s.init_from_argmax(case.phi, case.alpha)
+        s.prestep()
+        s.step(warm)
+        s.sync()
+        with ClockSampler(0) as clk:
+            ms = s.time_steps(steps)
+        over = s.overflow_cells()
+        torch.cuda.synchronize()
+    per = ms / steps
+    # end to end through the C ABI with host buffers
+    t0 = time.perf_counter()
+    with DenseSolver(case) as s:
+        s.init_from_argmax(case.phi, case.alpha)
+        s.prestep()
+        s.step(warm + steps)
+        phi, alpha = s.collect(clear=True)
+    e2e_s = time.perf_counter() - t0
+    # the reference's kernels on the same initial state
+    ref = None
+    try:
+        from oracle import DenseOracle, RefDenseGPU
+        rg = RefDenseGPU()
+        rg.check(rg.L.refd_set_params(p, R))
+        ph0 = DenseOracle().ini(p, case.phi, case.alpha)
+        dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        a, b = dev(ph0), dev(ph0)
+        x, y, z = (dev(np.asarray(v, np.float32)) for v in (case.x, case.y, case.z))
+        si, co = dev(np.asarray(case.sint, np.float32)), dev(np.asarray(case.cost, np.float32))
+        rms = C.c_float()
+        argv = (x.data_ptr(), y.data_ptr(), z.data_ptr(), a.data_ptr(), b.data_ptr(), si.data_ptr(),
+                co.data_ptr(), C.byref(rms))
+        rg.check(rg.L.refd_run_steps(warm + (warm % 2), 0, *argv))
+        rg.check(rg.L.refd_run_steps(steps, warm + (warm % 2), *argv))
+        ref = {"ms_per_step": rms.value / steps, "what": "reference set_BC_3D + rhs_psi "
+               "(3DgrainMPI/PhaseField.cu) compiled for sm_100a, same case"}
+        del a, b
+        torch.cuda.empty_cache()
+    except FileNotFoundError as e:
+        ref = {"unavailable": str(e)}
+    with APTSolver(case, precision="fp32") as s:
+        s.init_from_argmax(case.phi, case.alpha)
+        s.step(warm)
+        s.sync()
+        apt_ms = s.time_steps(steps) / steps
+    nbytes = 8 * ng  # every grain's phi read once and written once
+    peak, src = measured_peak()
+    achieved = cells * nbytes / (per * 1e-3) / 1e9
+    out = {"metric": "3D full-PF (-a) Mcell-upd/s", "value": cells / per / 1e3, "unit": "Mcell-upd/s",
+           "n_gpus": 1, "steps": steps, "warmup": warm, "ms_per_step": per,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+           "data": "synthetic",
+           "config": {"workload": "3D full-PF line step %dx%dx%d interior, NUM_PF = %d grains"
+                                  % (nx, ny, nz, ng),
+                      "interior": [nx, ny, nz], "grains": ng, "seed": SEED,
+                      "l2": "phi buffers 2x%.0f MB" % (4 * ng * case.length / 1e6)},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "traffic": None, "peak_source": src,
+                        "algorithmic_bytes_per_cell": nbytes},
+           "reference_kernels": ref,
+           "speedup_vs_reference_kernels": (ref["ms_per_step"] / per) if "ms_per_step" in ref else None,
+           "apt_same_case": {"ms_per_step": apt_ms, "num_pf": NUM_PF,
+                             "speedup_apt_over_full_pf": per / apt_ms},
+           "overflow_cells_last_step": over,
+           "e2e": {"value": cells * (warm + steps) / e2e_s / 1e6, "unit": "Mcell-upd/s",
+                   "h2d_bytes_per_step": 8 * case.length / (warm + steps),
+                   "d2h_bytes_per_step": 8 * case.length / (warm + steps), "seconds": e2e_s},
+           "cpu_baseline": None if args.no_cpu_baseline else dense_cpu_baseline(case),
+           "clocks": clk.summary(), "gpu_launches": 2 * steps}
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -381,8 +494,9 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp16"])
     ap.add_argument("--interior", type=int, nargs=3, metavar=("NX", "NY", "NZ"),
                     help="smaller line case for profiling (grains scale with the xy area)")
-    ap.add_argument("--workload", default="apt3d", choices=["apt3d", "ek2d"],
-                    help="ek2d: the split-precision 2D dendrite benchmark")
+    ap.add_argument("--workload", default="apt3d", choices=["apt3d", "ek2d", "dense"],
+                    help="ek2d: the split-precision 2D dendrite benchmark; dense: the full-PF "
+                         "(-a) mode against the reference kernels and the APT step")
     ap.add_argument("--ek2d-grid", type=int, nargs=2, metavar=("NX", "NY"))
     ap.add_argument("--ek2d-steps", type=int, default=EK2D_STEPS)
     args = ap.parse_args()
@@ -398,6 +512,8 @@ def main():
         return run_serve(args)
     if args.workload == "ek2d":
         return run_ek2d(args)
+    if args.workload == "dense":
+        return run_dense(args)
 
     import torch
     from cupf_b200.solver import APTSolver

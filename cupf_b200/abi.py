@@ -124,6 +124,24 @@ def lib():
                                              C.POINTER(C.c_uint8), C.POINTER(C.c_int32), C.c_int],
             "cupf_grain_volumes_noalloc": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                            C.POINTER(C.c_int64), vp],
+            "cupf_dense_create": [C.POINTER(cupf_apt_params), C.POINTER(cupf_apt_inputs), C.c_float,
+                                  C.c_int, C.POINTER(vp)],
+            "cupf_dense_destroy": [vp],
+            "cupf_dense_init_from_argmax": [vp, FP, C.POINTER(C.c_int32)],
+            "cupf_dense_prestep": [vp],
+            "cupf_dense_step": [vp, C.c_int32],
+            "cupf_dense_steps_done": [vp, C.POINTER(C.c_int64)],
+            "cupf_dense_collect": [vp, C.c_int32, FP, C.POINTER(C.c_int32)],
+            "cupf_dense_get_slots": [vp, FP],
+            "cupf_dense_set_slots": [vp, FP, C.c_int64],
+            "cupf_dense_move_domain": [vp, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32),
+                                       C.POINTER(C.c_int32)],
+            "cupf_dense_get_archive": [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)],
+            "cupf_dense_get_z": [vp, FP],
+            "cupf_dense_sync": [vp, C.c_int32],
+            "cupf_dense_time_steps": [vp, C.c_int32, FP],
+            "cupf_dense_set_tuning": [vp, C.c_int32],
+            "cupf_dense_overflow_cells": [vp, C.POINTER(C.c_int64)],
             "cupf_server_create": [C.POINTER(cupf_server_config), C.POINTER(vp)],
             "cupf_server_destroy": [vp],
             "cupf_server_submit": [vp, C.POINTER(cupf_apt_params), C.POINTER(cupf_apt_inputs), FP,

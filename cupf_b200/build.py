@@ -19,7 +19,8 @@ EXE = os.path.join(HERE, "phase_field")
 EXE2D = os.path.join(HERE, "phase_field_2d")
 OBJ = os.path.join(HERE, "_build")
 CU_SOURCES = [os.path.join(HERE, "csrc", f)
-              for f in ("cupf_capi.cu", "cupf_server.cu", "cupf_noalloc.cu", "cupf_ek2d.cu")]
+              for f in ("cupf_capi.cu", "cupf_server.cu", "cupf_noalloc.cu", "cupf_ek2d.cu",
+                        "cupf_dense.cu")]
 CPP_SOURCES = [os.path.join(HERE, "host", f) for f in
                ("host_util.cpp", "qoi.cpp", "phase_field.cpp", "npz_writer.cpp", "host_capi.cpp",
                 "ek2d_host.cpp")]

@@ -9,6 +9,8 @@
 // compiled for sm_100a.  Site order and meaning match oracle/apt_oracle.c.
 #pragma once
 
+#include <type_traits>
+
 #include "apt_common.cuh"
 
 namespace cupf {
@@ -21,6 +23,15 @@ struct Contract {
   static constexpr int AS = 1, UX_IN = 1, UX_OUT = 1, UY = 2, UZ_IN = 1, UZ_OUT = 1,
                        MAG_IN = 0, MAG_OUT = 0, Q_IN = 2, Q_OUT = 1, DIFF = 1, REP = 1, W = 1,
                        E1 = 2, INNER = 1, RHS = 1, NEW = 1, TD = 1;
+};
+
+// The full-PF kernel (PhaseField.cu:168-301), pinned the same way against its own
+// dumps: the sums of its rotation (X/Y/Z, PhaseField.cu:37-44) and, of the sums it
+// shares in shape with the APT kernel, the quartic and E1 sums fused on the other
+// side.
+struct ContractFull : Contract {
+  static constexpr int Q_IN = 1, E1 = 1;
+  static constexpr int X_IN = 2, X_OUT = 1, Y_IN = 2, Y_OUT = 1, Z_OUT = 1;
 };
 
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
@@ -54,25 +65,25 @@ __device__ __forceinline__ KineConst kine_const(float kd) {
 //   ( ca*cb*ux + sa*cb*uy - sb*uz,  -sa*ux + ca*uy + 0,  ca*sb*ux + sa*sb*uy + cb*uz );
 // full-PF kernel (kFull, PhaseField.cu:37-44), a different rotation:
 //   ( ca*cb*ux + sa*uy + ca*sb*uz,  -sa*cb*ux + ca*uy - sa*sb*uz,  -sb*ux + 0 + cb*uz ).
-// The full-PF sums take the fusions of the APT sums of the same shape.
 template <bool kFull>
 __device__ __forceinline__ void rotate_normal(float ux, float uy, float uz, float cosa, float sina,
                                               float cosb, float sinb, float& rx, float& ry,
                                               float& rz) {
-  using K = Contract;
   if (!kFull) {
+    using K = Contract;
     float s = sop<K::UX_IN>(fmul(cosa, cosb), ux, fmul(sina, cosb), uy);
     rx = K::UX_OUT ? ffma(-sinb, uz, s) : fsub(s, fmul(sinb, uz));
     ry = fadd(sop<K::UY>(-sina, ux, cosa, uy), 0.0f);
     s = sop<K::UZ_IN>(fmul(cosa, sinb), ux, fmul(sina, sinb), uy);
     rz = K::UZ_OUT ? ffma(cosb, uz, s) : fadd(s, fmul(cosb, uz));
   } else {
-    float s = sop<K::UX_IN>(fmul(cosa, cosb), ux, sina, uy);
-    rx = K::UX_OUT ? ffma(fmul(cosa, sinb), uz, s) : fadd(s, fmul(fmul(cosa, sinb), uz));
-    s = sop<K::UX_IN>(fmul(-sina, cosb), ux, cosa, uy);
-    ry = K::UX_OUT ? ffma(-fmul(sina, sinb), uz, s) : fsub(s, fmul(fmul(sina, sinb), uz));
+    using K = ContractFull;
+    float s = sop<K::X_IN>(fmul(cosa, cosb), ux, sina, uy);
+    rx = K::X_OUT ? ffma(fmul(cosa, sinb), uz, s) : fadd(s, fmul(fmul(cosa, sinb), uz));
+    s = sop<K::Y_IN>(fmul(-sina, cosb), ux, cosa, uy);
+    ry = K::Y_OUT ? ffma(-fmul(sina, sinb), uz, s) : fsub(s, fmul(fmul(sina, sinb), uz));
     s = fadd(fmul(-sinb, ux), 0.0f);
-    rz = K::UZ_OUT ? ffma(cosb, uz, s) : fadd(s, fmul(cosb, uz));
+    rz = K::Z_OUT ? ffma(cosb, uz, s) : fadd(s, fmul(cosb, uz));
   }
 }
 
@@ -81,7 +92,7 @@ __device__ __forceinline__ void rotate_normal(float ux, float uy, float uz, floa
 template <bool kFull = false>
 __device__ __forceinline__ float kine_ani(float ux, float uy, float uz, float cosa, float sina,
                                           float cosb, float sinb, KineConst kc, float eps) {
-  using K = Contract;
+  using K = typename std::conditional<kFull, ContractFull, Contract>::type;
   const float a_s = kc.a_s, epsilon = kc.epsilon;
   float rx, ry, rz;
   rotate_normal<kFull>(ux, uy, uz, cosa, sina, cosb, sinb, rx, ry, rz);
@@ -177,7 +188,7 @@ template <bool kFull = false, class A>
 __device__ __forceinline__ float slot_update(const A& a, KineConst kc, const float ph[7],
                                              float sina, float cosa, float sinb, float cosb,
                                              float repul, float Up) {
-  using K = Contract;
+  using K = typename std::conditional<kFull, ContractFull, Contract>::type;
   const float phD = ph[0], phB = ph[1], phL = ph[2], phC = ph[3], phR = ph[4], phT = ph[5],
               phU = ph[6];
   float phx = fmul(fsub(phR, phL), 0.5f);

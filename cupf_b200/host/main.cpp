@@ -15,11 +15,9 @@ int main(int argc, char** argv) {
     std::fprintf(stderr, "%s\n", err.c_str());
     return 2;
   }
-  if (!ds.useAPT) {
-    std::fprintf(stderr, "the full (non-APT) phase-field mode is not built\n");
-    return 2;
-  }
-  std::unique_ptr<APTPhaseField> pf(new APTPhaseField());
+  // -a selects the full (non-APT) solver, one phi field per grain (main.cpp:39-47)
+  std::unique_ptr<PhaseField> pf(ds.useAPT ? static_cast<PhaseField*>(new APTPhaseField())
+                                           : new PhaseField());
   pf->SetDesignSetting(&ds);
   pf->mac.folder = ds.thermalInputFolder + std::to_string(ds.seedValue);
   pf->params.seed_val = ds.seedValue;

@@ -3,6 +3,7 @@
 
 #include <getopt.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -71,7 +72,14 @@ void MovingDomain::allocateMovingDomain(int numGrains, int movingDirectionSize) 
 }
 
 // ------------------------------------------------------------------ PhaseField
-PhaseField::~PhaseField() = default;
+PhaseField::~PhaseField() {
+  if (mDense) cupf_dense_destroy(mDense);
+}
+
+bool PhaseField::check(cupf_status st, const char* what) {
+  if (st == CUPF_OK) return true;
+  return setErr(std::string(what) + ": " + cupf_last_error());
+}
 
 QoiGrid PhaseField::qoiGrid() const {
   QoiGrid g;
@@ -422,12 +430,8 @@ APTPhaseField::~APTPhaseField() {
   if (mHandle) cupf_apt_destroy(mHandle);
 }
 
-bool APTPhaseField::check(cupf_status st, const char* what) {
-  if (st == CUPF_OK) return true;
-  return setErr(std::string(what) + ": " + cupf_last_error());
-}
 
-cupf_apt_params APTPhaseField::deviceParams() const {
+cupf_apt_params PhaseField::deviceParams() const {
   const GlobalConstants& p = params;
   cupf_apt_params d;
   std::memset(&d, 0, sizeof(d));
@@ -595,6 +599,76 @@ bool APTPhaseField::evolve() {
   params.walltime =
       (int)std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   params.Mt = 2 * kt;
+  return true;
+}
+
+// PhaseField::cudaSetup (PhaseField.cu:431-493): the full-PF solver, one phi field
+// per grain (params.NUM_PF = params.num_theta, :440).
+bool PhaseField::cudaSetup() {
+  params.NUM_PF = params.num_theta;
+  NUM_PF = params.NUM_PF;
+  cupf_apt_params d = deviceParams();
+  cupf_apt_inputs in;
+  std::memset(&in, 0, sizeof(in));
+  in.x = x.data();
+  in.y = y.data();
+  in.z = z.data();
+  in.sint = mac.sint.data();
+  in.cost = mac.cost.data();
+  return check(cupf_dense_create(&d, &in, params.R, device, &mDense), "cupf_dense_create");
+}
+
+// PhaseField::evolve (PhaseField.cu:495-632) without MPI: line QoIs every Mt/nts
+// steps and the moving-domain check every TIPP steps, whatever the -l flag (the
+// full-PF evolve does both unconditionally).  The reference's last update of the
+// loop (:604) writes a buffer nothing reads afterwards (the final collect_PF at
+// :617 reads the other one), so the loop stops before it.
+bool PhaseField::evolve() {
+  const DesignSettingData* ds = GetSetDesignSetting();
+  if (ds && ds->includeNucleation) return setErr("the full-PF mode has no nucleation");
+  if (!mDense) return setErr("cudaSetup has not run");
+  MovingDomain md;
+  md.allocateMovingDomain(params.num_theta, fnz);
+  md.tip_thres = (int)((1 - 0.2) * fnz);  // (1-BLANK)*fnz, PhaseField.cu:517
+  if (!check(cupf_dense_init_from_argmax(mDense, phi.data(), alpha.data()), "init")) return false;
+  if (!check(cupf_dense_prestep(mDense), "prestep")) return false;
+  md.cur_tip = 1;
+  qois->calculateLineQoIs(qoiGrid(), md.cur_tip, alpha.data(), 0, z.data(),
+                          md.loss_area_host.data(), md.move_count);
+  const int kts = params.nts > 0 ? params.Mt / params.nts : 0;
+  const int kt_max = params.Mt / 2;
+  auto t0 = std::chrono::steady_clock::now();
+  for (int kt = 0; kt < kt_max; kt++) {
+    if (!check(cupf_dense_step(mDense, 1), "cupf_dense_step")) return false;
+    if (kts > 0 && (2 * kt + 2) % kts == 0) {
+      if (!check(cupf_dense_collect(mDense, 1, nullptr, alpha.data()), "collect") ||
+          !check(cupf_dense_get_archive(mDense, 0, nullptr, md.loss_area_host.data()), "archive") ||
+          !check(cupf_dense_get_z(mDense, z.data()), "z"))
+        return false;
+      md.cur_tip = 0;
+      qois->calculateLineQoIs(qoiGrid(), md.cur_tip, alpha.data(), (2 * kt + 2) / kts, z.data(),
+                              md.loss_area_host.data(), md.move_count);
+    }
+    if ((2 * kt + 2) % kTIPP == 0) {
+      int moved = 0;
+      if (!check(cupf_dense_move_domain(mDense, &md.tip_front, md.tip_thres, &md.move_count, &moved),
+                 "cupf_dense_move_domain"))
+        return false;
+    }
+    if (kt + 1 < kt_max && !check(cupf_dense_step(mDense, 1), "cupf_dense_step")) return false;
+  }
+  if (!check(cupf_dense_collect(mDense, 1, phi.data(), alpha.data()), "collect")) return false;
+  if (fnz_f > 0 && !alpha_i_full.empty()) {
+    if (!check(cupf_dense_get_archive(mDense, fnz_f, alpha_i_full.data(), nullptr), "archive"))
+      return false;
+    const long long off = (long long)md.move_count * fnx * fny;
+    if (off < full_length)
+      std::memcpy(alpha_i_full.data() + off, alpha.data(),
+                  sizeof(int) * std::min<long long>(length, full_length - off));
+  }
+  if (!check(cupf_dense_sync(mDense, 0), "sync")) return false;
+  params.walltime =
+      (int)std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return true;
 }
 

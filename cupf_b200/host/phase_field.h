@@ -3,8 +3,9 @@
 // Class and method names, call order and input semantics follow the reference
 // driver (3DgrainMPI/main.cpp:15-77, PhaseField.h:11-59, APTPhaseField.h:11-30,
 // DesignSettingData.h, MovingDomain.h, ThermalInputData.h); the device work
-// goes through the C ABI of include/cupf.h.  One process drives one GPU (the
-// reference's MPI slabs are replaced by a whole-domain solver).
+// goes through the C ABI of include/cupf.h (include/cupf_dense.h for -a).  One
+// process drives one GPU (the reference's MPI slabs are replaced by a
+// whole-domain solver).
 #pragma once
 
 #include <memory>
@@ -12,6 +13,7 @@
 #include <vector>
 
 #include "../../include/cupf.h"
+#include "../../include/cupf_dense.h"
 #include "qoi.h"
 
 namespace cupf_host {
@@ -91,6 +93,9 @@ class MovingDomain {
   std::vector<int> loss_area_host;
 };
 
+// The full (non-APT) phase-field solver, one phi field per grain (the reference's
+// PhaseField, PhaseField.cu:431-632, selected by -a); APTPhaseField overrides
+// cudaSetup and evolve with the active-parameter-tracking solver.
 class PhaseField {
  public:
   virtual ~PhaseField();
@@ -98,8 +103,8 @@ class PhaseField {
   bool parseInputParams(const std::string& fileName);
   bool cpuSetup();
   bool initField();
-  virtual bool cudaSetup() = 0;
-  virtual bool evolve() = 0;
+  virtual bool cudaSetup();
+  virtual bool evolve();
   // Device candidates of the 3D junction search on the last collected argmax map
   // (cells ascending, per-cell distinct counts); false where there are none.
   virtual bool deviceJunctionCandidates(std::vector<long long>&, std::vector<unsigned char>&) {
@@ -120,14 +125,18 @@ class PhaseField {
   std::unique_ptr<QOI> qois;
   QoiGrid qoiGrid() const;
   std::string outputBaseName() const;
+  cupf_apt_params deviceParams() const;
+  int device = 0;
 
  protected:
   bool setErr(const std::string& e) {
     mErr = e;
     return false;
   }
+  bool check(cupf_status st, const char* what);
   const DesignSettingData* mDesignSetting = nullptr;
   std::string mErr;
+  cupf_dense_handle* mDense = nullptr;
 };
 
 class APTPhaseField : public PhaseField {
@@ -138,15 +147,12 @@ class APTPhaseField : public PhaseField {
   bool deviceJunctionCandidates(std::vector<long long>& cells,
                                 std::vector<unsigned char>& distinct) override;
   cupf_apt_handle* handle() const { return mHandle; }
-  cupf_apt_params deviceParams() const;
-  int device = 0;
   cupf_precision precision = CUPF_PREC_FP32;
 
  protected:
   bool moveDomain(MovingDomain* md);
   bool getLineQoIs(MovingDomain* md);
   bool collectToHost(bool clear);
-  bool check(cupf_status st, const char* what);
   cupf_apt_handle* mHandle = nullptr;
 };
 

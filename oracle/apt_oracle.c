@@ -15,6 +15,8 @@
  *   oracle_ini                 APTini_PF             3DgrainMPI/APTPhaseField.cu:78-89
  *   oracle_move_frame          APTmove_frame+APTcopy_frame  3DgrainMPI/APTPhaseField.cu:357-410
  *   oracle_tip_scan            ave_x + tip_mvf       3DgrainMPI/PhaseField.cu:366-399
+ * and the full (non-APT, -a) mode of PhaseField.cu in the last section
+ * (oracle_dense_*: set_BC_3D, rhs_psi, collect_PF, ini_PF, move/copy_frame).
  *
  * Two arithmetic modes:
  *   f32: single precision with the same operation order as the reference source.
@@ -657,4 +659,192 @@ int oracle_nucleate(const cupf_apt_params* p, const cupf_apt_inputs* th, float* 
     count++;
   }
   return count;
+}
+
+/* ---------------------------------------------------------------- full-PF mode
+ * The dense solver of PhaseField (3DgrainMPI/PhaseField.cu), one phi field per
+ * grain, NUM_PF = num_theta, reference layout ph[g*length + C]:
+ *   oracle_dense_set_bc     set_BC_3D   PhaseField.cu:111-166 (mirror on every face)
+ *   oracle_dense_rhs_f32    rhs_psi     PhaseField.cu:168-301, kine_ani :32-50
+ *   oracle_dense_collect    collect_PF  PhaseField.cu:60-88 (persistent argmax)
+ *   oracle_dense_ini        set_minus1 + ini_PF  PhaseField.cu:51-57, 91-107
+ *   oracle_dense_move_frame move_frame + copy_frame  PhaseField.cu:316-363
+ * The sums of the full-PF rotation are switched like the APT sites (g_dcfg); the
+ * sites of the same shape as the APT kernel's (a_s, magnitude, quartic,
+ * diffusion, repulsion, update) have switches of their own (g_dsh), pinned
+ * separately against dumps of the full-PF kernels. */
+enum {
+  D_X_IN = 0, /* (ca*cb)*ux + sa*uy                  : 0/1/2 */
+  D_X_OUT,    /* s + (ca*sb)*uz                      : 0/1 */
+  D_Y_IN,     /* ((-sa)*cb)*ux + ca*uy               : 0/1/2 */
+  D_Y_OUT,    /* s - (sa*sb)*uz                      : 0/1 */
+  D_Z_OUT,    /* ((-sb)*ux + 0) + cb*uz              : 0/1 */
+  D_TD,       /* z - (R*1e6)*t in double             : 0/1 */
+  D_NSITES
+};
+static int g_dcfg[D_NSITES] = {1, 1, 1, 1, 1, 1};
+/* the sites the full-PF kernel shares with the APT one, switched separately
+ * (nvcc fuses some of them differently in the two kernels) */
+static int g_dsh[S_NSITES] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
+
+/* D_NSITES full-PF sites followed by S_NSITES shared ones */
+int oracle_dense_num_sites(void) { return D_NSITES + S_NSITES; }
+void oracle_dense_set_contraction(const int32_t* cfg, int n) {
+  for (int i = 0; i < n && i < D_NSITES + S_NSITES; ++i) {
+    if (i < D_NSITES) g_dcfg[i] = cfg[i];
+    else g_dsh[i - D_NSITES] = cfg[i];
+  }
+}
+
+static float kine_ani_full_f32(float ux, float uy, float uz, float cosa, float sina, float cosb,
+                               float sinb, float kd, float eps) {
+  float a_s = g_dsh[S_AS] ? fmaf(3.0f, kd, 1.0f) : 1.0f + 3.0f * kd;
+  float epsilon = -4.0f * kd / a_s;
+  float s = sop(cosa * cosb, ux, sina, uy, g_dcfg[D_X_IN]);
+  float rx = g_dcfg[D_X_OUT] ? fmaf(cosa * sinb, uz, s) : s + (cosa * sinb) * uz;
+  s = sop(-sina * cosb, ux, cosa, uy, g_dcfg[D_Y_IN]);
+  float ry = g_dcfg[D_Y_OUT] ? fmaf(-(sina * sinb), uz, s) : s - (sina * sinb) * uz;
+  s = (-sinb * ux) + 0.0f;
+  float rz = g_dcfg[D_Z_OUT] ? fmaf(cosb, uz, s) : s + cosb * uz;
+  float ux2 = rx * rx, uy2 = ry * ry, uz2 = rz * rz;
+  float mag = sop(rx, rx, ry, ry, g_dsh[S_MAG_IN]);
+  mag = g_dsh[S_MAG_OUT] ? fmaf(rz, rz, mag) : mag + uz2;
+  float mag2 = mag * mag;
+  if (mag > eps) {
+    float q = sop(ux2, ux2, uy2, uy2, g_dsh[S_Q_IN]);
+    q = g_dsh[S_Q_OUT] ? fmaf(uz2, uz2, q) : q + uz2 * uz2;
+    return a_s * (1.0f + epsilon * q / mag2);
+  }
+  return 1.0f;
+}
+
+void oracle_dense_set_bc(const cupf_apt_params* p, float* ph) {
+  const int fnx = p->fnx, fny = p->fny, fnz = p->fnz, np = p->num_theta;
+  const int64_t len = (int64_t)fnx * fny * fnz;
+  for (int g = 0; g < np; ++g)
+    for (int k = 0; k < fnz; ++k)
+      for (int j = 0; j < fny; ++j)
+        for (int i = 0; i < fnx; ++i) {
+          int hk = (k == 0 || k == fnz - 1), hj = (j == 0 || j == fny - 1),
+              hi = (i == 0 || i == fnx - 1);
+          if (!(hk || hj || hi)) continue;
+          int si = bc_map(i, fnx, 0), sj = bc_map(j, fny, 0), sk = bc_map(k, fnz, 0);
+          ph[g * len + i + (int64_t)j * fnx + (int64_t)k * fnx * fny] =
+              ph[g * len + si + (int64_t)sj * fnx + (int64_t)sk * fnx * fny];
+        }
+}
+
+/* rhs_psi of every grain at every interior cell from a buffer whose halo is
+ * filled; t in seconds, R = Rmax in m/s. */
+void oracle_dense_rhs_f32(const cupf_apt_params* p, const float* z, const float* sint,
+                          const float* cost, float R, float t, const float* ph, float* ph_new) {
+  const int fnx = p->fnx, fny = p->fny, fnz = p->fnz, np = p->num_theta;
+  const int64_t len = (int64_t)fnx * fny * fnz, sx = 1, sy = fnx, sz = (int64_t)fnx * fny;
+  const double Rm = (double)R * 1e6;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int k = 1; k < fnz - 1; ++k)
+    for (int j = 1; j < fny - 1; ++j) {
+      /* Tinterp = cP.G*(z[k] - cP.R*1e6*t - 2) in double (PhaseField.cu:277) */
+      double r = g_dcfg[D_TD] ? fma(-Rm, (double)t, (double)z[k]) : (double)z[k] - Rm * (double)t;
+      float Tinterp = (float)((double)p->G * (r - 2.0));
+      float Up = Tinterp / p->L_cp;
+      for (int i = 1; i < fnx - 1; ++i) {
+        int64_t C0 = i + (int64_t)j * sy + (int64_t)k * sz;
+        for (int g = 0; g < np; ++g) {
+          int64_t C = C0 + g * len;
+          float phC = ph[C], phR = ph[C + sx], phL = ph[C - sx], phT = ph[C + sy],
+                phB = ph[C - sy], phU = ph[C + sz], phD = ph[C - sz];
+          float phxn = (phR - phL) * 0.5f, phyn = (phT - phB) * 0.5f, phzn = (phU - phD) * 0.5f;
+          float cosa, sina, cosb, sinb;
+          if ((double)phC > LS) {
+            sina = sint[g + 1];
+            cosa = cost[g + 1];
+            sinb = sint[g + 1 + np];
+            cosb = cost[g + 1 + np];
+          } else {
+            sina = 0.0f;
+            cosa = 1.0f;
+            sinb = 0.0f;
+            cosb = 1.0f;
+          }
+          float A2 = kine_ani_full_f32(phxn, phyn, phzn, cosa, sina, cosb, sinb, p->kin_delta,
+                                       p->eps);
+          float sum = phR + phL + phT + phB + phU + phD;
+          float diff = g_dsh[S_DIFF] ? fmaf(-6.0f, phC, sum) : sum - 6.0f * phC;
+          float repul = 0.0f;
+          for (int b = 0; b < np; ++b) {
+            if (b == g) continue;
+            float q = ph[C0 + b * len] + 1.0f;
+            repul = g_dsh[S_REP] ? fmaf(0.25f * q, q, repul) : repul + 0.25f * q * q;
+          }
+          float w = g_dsh[S_W] ? fmaf(-phC, phC, 1.0f) : 1.0f - phC * phC;
+          float dh = diff * p->hi;
+          float E1 = sop(dh, p->hi, w, phC, g_dsh[S_E1]);
+          float m6 = 6.0f * (phC + 1.0f);
+          float inner;
+          if (g_dsh[S_INNER] == 1) inner = fmaf(w, w, -(m6 * repul));
+          else if (g_dsh[S_INNER] == 2) inner = fmaf(-m6, repul, w * w);
+          else inner = w * w - m6 * repul;
+          float lu = p->lamd * Up;
+          float rhs = g_dsh[S_RHS] ? fmaf(-lu, inner, E1) : E1 - lu * inner;
+          float dphi = rhs / A2;
+          ph_new[C] = g_dsh[S_NEW] ? fmaf(p->dt, dphi, phC) : phC + p->dt * dphi;
+        }
+      }
+    }
+}
+
+/* argmax starts from argmax[C] and moves only to a strictly larger grain; phi /
+ * alpha written only where the max is above LS */
+void oracle_dense_collect(const cupf_apt_params* p, const float* ph, float* phi, int32_t* alpha,
+                          int32_t* argmax) {
+  const int np = p->num_theta;
+  const int64_t len = (int64_t)p->fnx * p->fny * p->fnz;
+  for (int64_t C = 0; C < len; ++C) {
+    for (int g = 0; g < np; ++g)
+      if (ph[C + g * len] > ph[C + (int64_t)argmax[C] * len]) argmax[C] = g;
+    float v = ph[C + (int64_t)argmax[C] * len];
+    if ((double)v > LS) {
+      phi[C] = v;
+      alpha[C] = argmax[C] + 1;
+    }
+  }
+}
+
+void oracle_dense_ini(const cupf_apt_params* p, float* ph, const float* phi, const int32_t* alpha) {
+  const int np = p->num_theta;
+  const int64_t len = (int64_t)p->fnx * p->fny * p->fnz;
+  for (int64_t C = 0; C < (int64_t)np * len; ++C) ph[C] = -1.0f;
+  for (int64_t C = 0; C < len; ++C)
+    if ((double)phi[C] > LS && alpha[C] >= 1 && alpha[C] <= np) ph[C + (alpha[C] - 1) * len] = phi[C];
+}
+
+/* move_frame + copy_frame: interior k <- k+1, the top interior layer 2*phi[top] -
+ * phi[top-1], archive and lost area as oracle_move_frame. */
+void oracle_dense_move_frame(const cupf_apt_params* p, float* ph, float* z, const int32_t* alpha,
+                             int32_t* alpha_full, int32_t* loss_area, int move_count) {
+  const int fnx = p->fnx, fny = p->fny, fnz = p->fnz, np = p->num_theta;
+  const int64_t plane = (int64_t)fnx * fny, len = plane * fnz;
+  for (int64_t c = 0; c < plane; ++c) {
+    int32_t a = alpha[plane + c];
+    alpha_full[(int64_t)move_count * plane + plane + c] = a;
+    if (a >= 1 && a <= p->num_theta) loss_area[a - 1] += 1;
+  }
+  float* top = (float*)malloc(sizeof(float) * (size_t)plane);
+  for (int g = 0; g < np; ++g) {
+    for (int64_t c = 0; c < plane; ++c) {
+      int64_t C = g * len + (fnz - 2) * plane + c;
+      top[c] = 2.0f * ph[C] - ph[C - plane];
+    }
+    for (int k = 1; k < fnz - 1; ++k)
+      for (int j = 1; j < fny - 1; ++j)
+        for (int i = 1; i < fnx - 1; ++i) {
+          int64_t C = g * len + k * plane + (int64_t)j * fnx + i;
+          ph[C] = (k < fnz - 2) ? ph[C + plane] : top[(int64_t)j * fnx + i];
+        }
+  }
+  free(top);
+  float ztop = 2.0f * z[fnz - 2] - z[fnz - 3];
+  for (int k = 1; k < fnz - 2; ++k) z[k] = z[k + 1];
+  z[fnz - 2] = ztop;
 }

@@ -9,6 +9,8 @@ Outputs
                                 ...) compiled for sm_100a, NUM_PF=5 as shipped,
                                 with launchers (ref/ref_harness.cu)
   oracle/_ref/libref_aptN.so    the same with APT_NUM_PF set to N (N = 1..8)
+  oracle/_ref/libref_dense.so   reference full-PF kernels (PhaseField.cu, unmodified)
+                                with launchers (ref/ref_dense_harness.cu)
   oracle/_ref/libref_ek2d.so    reference 2D line-model kernels and setup()
                                 (2DdendriteMPI/line_model/PF.cu, unmodified) with
                                 launchers (ref/ref_ek2d_harness.cu)
@@ -130,6 +132,45 @@ def build_ref_gpu(num_pf, force=False):
     return out
 
 
+def build_ref_dense(force=False):
+    """The reference's full-PF kernels (PhaseField.cu, unmodified, from REF_DIR)
+    with the launchers of ref/ref_dense_harness.cu, in a library of their own: the
+    harness includes PhaseField.cu to reach its kernels and its __constant__
+    parameters, so PhaseField's methods are compiled here and nowhere else in it."""
+    if not os.path.isdir(REF_DIR):
+        return None
+    os.makedirs(OUT, exist_ok=True)
+    out = os.path.join(OUT, "libref_dense.so")
+    harness = os.path.join(HERE, "ref", "ref_dense_harness.cu")
+    cu = [harness, os.path.join(REF_DIR, "MPIsettingCuda.cu")]
+    cpp = [os.path.join(REF_DIR, f) for f in ("helper.cpp", "QOI.cpp", "MovingDomain.cpp",
+                                                 "MPIsetting.cpp", "DesignSettingData.cpp",
+                                                 "ThermalInputData.cpp")]
+    cpp.append(os.path.join(HERE, "ref", "ref_host_stubs.cpp"))
+    deps = cu + cpp + [os.path.join(REF_DIR, "PhaseField.cu"), __file__,
+                       os.path.join(HERE, "ref", "mpi.h"), os.path.join(ROOT, "include", "cupf.h")]
+    if not force and _newer(out, deps):
+        return out
+    objdir = os.path.join(OUT, "obj_dense")
+    os.makedirs(objdir, exist_ok=True)
+    common = ["-I", os.path.join(HERE, "ref"), "-I", REF_DIR]
+    jobs = []
+    for s in cu:
+        o = os.path.join(objdir, os.path.basename(s) + ".o")
+        jobs.append([NVCC] + ARCH + ["-O3", "-std=c++14", "-w", "-Xcompiler", "-fPIC",
+                                     "-lineinfo", "-c", s, "-o", o] + common)
+    for s in cpp:
+        o = os.path.join(objdir, os.path.basename(s) + ".o")
+        jobs.append(["g++", "-O3", "-std=c++14", "-w", "-fPIC", "-c", s, "-o", o, "-I",
+                     CUDA_INC] + common)
+    with ThreadPoolExecutor(max_workers=8) as ex:
+        list(ex.map(_run, jobs))
+    objs = [j[j.index("-o") + 1] for j in jobs]
+    _run([NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", out] + objs +
+         ["-lcudart", "-lcurand", "-Xlinker", "--no-undefined"])
+    return out
+
+
 def build_ref_ek2d(force=False):
     """The reference's 2D line-model kernels (PF.cu, unmodified, from REF2D_DIR)
     with the launchers of ref/ref_ek2d_harness.cu."""
@@ -152,6 +193,7 @@ def build_all(force=False):
     outs = [build_oracle(force)]
     outs.append(build_ref_host(force))
     outs.append(build_ref_ek2d(force))
+    outs.append(build_ref_dense(force))
     with ThreadPoolExecutor(max_workers=2) as ex:
         outs += list(ex.map(lambda n: build_ref_gpu(n, force), range(1, 9)))
     return outs
