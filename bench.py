@@ -391,10 +391,18 @@ def dense_cpu_baseline(case, budget_s=15.0):
 
 
 def run_dense(args):
-    """The full (non-APT, -a) mode: one phi field per grain.  The library's
-    two-launch step, the reference's own set_BC_3D + rhs_psi pair on the same
-    state, and the APT step on the same case (the speed-up the -a comparison is
-    for), each timed on the device after warm-up steps from the initial state."""
+    """The full (non-APT, -a) mode: one phi field per grain.  The library's step
+    (one launch that evaluates the grains present near each cell and writes the
+    next step's per-cell lists), the reference's own set_BC_3D + rhs_psi pair on
+    the same state, and the APT step on the same case (the speed-up the -a
+    comparison is for), each timed on the device after warm-up steps from the
+    initial state.
+
+    Roofline bytes of the library's step: per interior cell its list count read
+    and written (8 B), and per grain that is not -1 at the cell its list entry read
+    and written (2 x 6 B), its value written and its previous value reset (2 x 4 B)
+    -- 20 B per present (cell, grain) pair, counted from the state.  The reference
+    reads and writes every grain of every cell (8 B x grains per cell)."""
     import ctypes as C
     import torch
     from cupf_b200 import cases
@@ -407,16 +415,23 @@ def run_dense(args):
     cells = nx * ny * nz
     R = case.meta["R"]
     steps, warm = args.steps, max(args.warmup, 3)
+    def present_pairs(ph):
+        a = ph.reshape(ng, p.fnz, p.fny, p.fnx)[:, 1:-1, 1:-1, 1:-1]
+        return int(np.count_nonzero(a != -1.0))
+
     with DenseSolver(case) as s:
         s.init_from_argmax(case.phi, case.alpha)
         s.prestep()
         s.step(warm)
         s.sync()
+        pairs0 = present_pairs(s.get_slots())
         with ClockSampler(0) as clk:
             ms = s.time_steps(steps)
         over = s.overflow_cells()
+        pairs1 = present_pairs(s.get_slots())
         torch.cuda.synchronize()
     per = ms / steps
+    pairs = 0.5 * (pairs0 + pairs1)
     # end to end through the C ABI with host buffers
     t0 = time.perf_counter()
     with DenseSolver(case) as s:
@@ -452,7 +467,7 @@ def run_dense(args):
         s.step(warm)
         s.sync()
         apt_ms = s.time_steps(steps) / steps
-    nbytes = 8 * ng  # every grain's phi read once and written once
+    nbytes = 8 + 20 * pairs / cells  # per cell-update, see the docstring
     peak, src = measured_peak()
     achieved = cells * nbytes / (per * 1e-3) / 1e9
     out = {"metric": "3D full-PF (-a) Mcell-upd/s", "value": cells / per / 1e3, "unit": "Mcell-upd/s",
@@ -465,7 +480,9 @@ def run_dense(args):
                       "l2": "phi buffers 2x%.0f MB" % (4 * ng * case.length / 1e6)},
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                         "frac": achieved / peak, "traffic": None, "peak_source": src,
-                        "algorithmic_bytes_per_cell": nbytes},
+                        "algorithmic_bytes_per_cell": nbytes,
+                        "present_grains_per_cell": pairs / cells,
+                        "full_pf_bytes_per_cell": 8 * ng},
            "reference_kernels": ref,
            "speedup_vs_reference_kernels": (ref["ms_per_step"] / per) if "ms_per_step" in ref else None,
            "apt_same_case": {"ms_per_step": apt_ms, "num_pf": NUM_PF,
@@ -475,7 +492,7 @@ def run_dense(args):
                    "h2d_bytes_per_step": 8 * case.length / (warm + steps),
                    "d2h_bytes_per_step": 8 * case.length / (warm + steps), "seconds": e2e_s},
            "cpu_baseline": None if args.no_cpu_baseline else dense_cpu_baseline(case),
-           "clocks": clk.summary(), "gpu_launches": 2 * steps}
+           "clocks": clk.summary(), "gpu_launches": steps}
     print(json.dumps(out))
     return 0
 

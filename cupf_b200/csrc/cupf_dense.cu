@@ -29,9 +29,11 @@ struct cupf_dense_handle {
   int cur = 0;                // buffer the next step reads
   bool halo_ok[2] = {false, false};
   int K = kDenseListMax;
-  int* cnt = nullptr;
-  unsigned short* lid = nullptr;
-  float* lval = nullptr;
+  // per-buffer lists of the grains that are not -1 at each cell (dense.cuh)
+  int* cnt[2] = {nullptr, nullptr};
+  unsigned short* lid[2] = {nullptr, nullptr};
+  float* lval[2] = {nullptr, nullptr};
+  bool list_ok[2] = {false, false};  // lists describe the buffer's current content
   unsigned long long* overflow = nullptr;
   float *x = nullptr, *y = nullptr, *z = nullptr, *orient = nullptr;
   std::vector<float> z_host;
@@ -56,7 +58,8 @@ int grid_for(long long n, int block = 256) {
 }
 
 void free_handle(cupf_dense_handle* h) {
-  void* ptrs[] = {h->buf[0], h->buf[1], h->cnt, h->lid, h->lval, h->overflow, h->x, h->y, h->z,
+  void* ptrs[] = {h->buf[0], h->buf[1], h->cnt[0], h->cnt[1], h->lid[0], h->lid[1], h->lval[0],
+                  h->lval[1], h->overflow, h->x, h->y, h->z,
                   h->orient, h->phi_m, h->alpha_m, h->argmax, h->layer_sums, h->alpha_full,
                   h->loss_area};
   for (void* p : ptrs)
@@ -88,9 +91,13 @@ cupf_status launch_step(cupf_dense_handle* h, float t) {
   const cupf_apt_params& p = h->p;
   const dim3 blk(32, 4);
   const dim3 grd((p.fnx - 2 + 31) / 32, (p.fny - 2 + 3) / 4, p.fnz - 2);
-  dense_list_kernel<<<grd, blk, 0, h->stream>>>(h->buf[h->cur], p.fnx, p.fny, p.fnz, h->np, h->K,
-                                                h->len, h->cnt, h->lid, h->lval);
-  CK(cudaGetLastError());
+  const int ci = h->cur, co = h->cur ^ 1;
+  if (!h->list_ok[ci]) {  // the state was replaced: lists from one read of every grain
+    dense_list_kernel<<<grd, blk, 0, h->stream>>>(h->buf[ci], p.fnx, p.fny, p.fnz, h->np, h->K,
+                                                  h->len, h->cnt[ci], h->lid[ci], h->lval[ci]);
+    CK(cudaGetLastError());
+    h->list_ok[ci] = true;
+  }
   CK(cudaMemsetAsync(h->overflow, 0, sizeof(unsigned long long), h->stream));
   DenseArgs a;
   std::memset(&a, 0, sizeof(a));
@@ -111,14 +118,19 @@ cupf_status launch_step(cupf_dense_handle* h, float t) {
   a.kin_delta = p.kin_delta;
   a.z = h->z;
   a.orient = reinterpret_cast<const float4*>(h->orient);
-  a.in = h->buf[h->cur];
-  a.out = h->buf[h->cur ^ 1];
-  a.cnt = h->cnt;
-  a.lid = h->lid;
-  a.lval = h->lval;
+  a.in = h->buf[ci];
+  a.out = h->buf[co];
+  a.cnt = h->cnt[ci];
+  a.lid = h->lid[ci];
+  a.lval = h->lval[ci];
+  a.cnt_o = h->cnt[co];
+  a.lid_o = h->lid[co];
+  a.lval_o = h->lval[co];
+  a.reset_from_lists = h->list_ok[co] ? 1 : 0;
   a.overflow = h->overflow;
   dense_update_kernel<<<grd, blk, 0, h->stream>>>(a);
   CK(cudaGetLastError());
+  h->list_ok[co] = true;
   h->cur ^= 1;
   h->halo_ok[h->cur] = false;
   return CUPF_OK;
@@ -183,11 +195,14 @@ extern "C" cupf_status cupf_dense_create(const cupf_apt_params* p, const cupf_ap
   TRY(cuda(cudaEventCreate(&h->ev1), "event"));
   const size_t fbytes = (size_t)h->len * h->np * sizeof(float);
   for (int b = 0; b < 2; ++b) TRY(cuda(cudaMalloc((void**)&h->buf[b], fbytes), "phi buffer"));
-  TRY(cuda(cudaMalloc((void**)&h->cnt, h->len * sizeof(int)), "list counts"));
-  TRY(cuda(cudaMemsetAsync(h->cnt, 0, h->len * sizeof(int), h->stream), "memset"));
-  TRY(cuda(cudaMalloc((void**)&h->lid, (size_t)kDenseListMax * h->len * sizeof(unsigned short)),
-           "lists"));
-  TRY(cuda(cudaMalloc((void**)&h->lval, (size_t)kDenseListMax * h->len * sizeof(float)), "lists"));
+  for (int b = 0; b < 2; ++b) {
+    TRY(cuda(cudaMalloc((void**)&h->cnt[b], h->len * sizeof(int)), "list counts"));
+    TRY(cuda(cudaMemsetAsync(h->cnt[b], 0, h->len * sizeof(int), h->stream), "memset"));
+    TRY(cuda(cudaMalloc((void**)&h->lid[b], (size_t)kDenseListMax * h->len * sizeof(unsigned short)),
+             "lists"));
+    TRY(cuda(cudaMalloc((void**)&h->lval[b], (size_t)kDenseListMax * h->len * sizeof(float)),
+             "lists"));
+  }
   TRY(cuda(cudaMalloc((void**)&h->overflow, sizeof(unsigned long long)), "overflow counter"));
   TRY(cuda(cudaMemsetAsync(h->overflow, 0, sizeof(unsigned long long), h->stream), "memset"));
   if (in->x) TRY(upload(&h->x, in->x, p->fnx, h->stream));
@@ -237,6 +252,7 @@ extern "C" cupf_status cupf_dense_init_from_argmax(cupf_dense_handle* h, const f
   CK(cudaStreamSynchronize(h->stream));
   h->cur = 0;
   h->halo_ok[0] = h->halo_ok[1] = false;
+  h->list_ok[0] = h->list_ok[1] = false;
   cupf_status st = fill_halo(h, 0);
   if (st) return st;
   if ((st = fill_halo(h, 1))) return st;
@@ -310,6 +326,7 @@ extern "C" cupf_status cupf_dense_set_slots(cupf_dense_handle* h, const float* p
                      cudaMemcpyHostToDevice, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   h->halo_ok[h->cur] = false;
+  h->list_ok[h->cur] = false;
   h->steps_done = steps_done;
   h->initialised = true;
   return CUPF_OK;
@@ -378,6 +395,7 @@ extern "C" cupf_status cupf_dense_move_domain(cupf_dense_handle* h, int32_t* tip
     CK(cudaStreamSynchronize(h->stream));
     h->halo_ok[h->cur] = false;
     h->halo_ok[h->cur ^ 1] = false;
+    h->list_ok[0] = h->list_ok[1] = false;
     *move_count += 1;
     *tip_front -= 1;
     *moved += 1;
@@ -451,6 +469,7 @@ extern "C" cupf_status cupf_dense_set_tuning(cupf_dense_handle* h, int32_t list_
   if (list_cap < 1 || list_cap > kDenseListMax)
     return cupf_fail(CUPF_ERR_INVALID, "list_cap=%d outside 1..%d", list_cap, kDenseListMax);
   h->K = list_cap;
+  h->list_ok[0] = h->list_ok[1] = false;  // lists hold at most the old capacity
   return CUPF_OK;
 }
 

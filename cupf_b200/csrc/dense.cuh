@@ -1,19 +1,24 @@
 // dense.cuh — kernels of the full (non-APT) phase-field mode: one phi field per
 // grain, phi[grain][z][y][x] in float (the reference's layout, PhaseField.cu).
 //
-// A step is two launches:
-//   dense_list_kernel    per interior cell, the grains whose phi differs from -1,
-//                        ascending, with their values (capacity K per cell; the
-//                        count is stored in full so a longer list is detected);
-//   dense_update_kernel  per interior cell, -1 into every grain of the output,
-//                        then the reference's update (rhs_psi, PhaseField.cu:168-301)
-//                        for each grain in the union of the seven stencil cells'
-//                        lists, with the repulsion summed over the centre list in
-//                        ascending grain order.
+// Each buffer has per-cell lists: the grains whose phi differs from -1 at the
+// cell, ascending, with their values (capacity K per cell; the count is stored in
+// full so a longer list is detected).  A step is one launch:
+//   dense_update_kernel  per interior cell: the grains the output buffer's lists
+//                        name (its content of two steps ago) are reset to -1, then
+//                        the reference's update (rhs_psi, PhaseField.cu:168-301) is
+//                        evaluated for each grain in the union of the seven stencil
+//                        cells' lists of the input buffer, with the repulsion summed
+//                        over the centre list in ascending grain order; the results
+//                        that differ from -1 form the output buffer's new lists.
 // Every grain outside that union is exactly -1 at all seven stencil points; its
 // update is exactly -1 and its repulsion term exactly zero, so skipping them
-// reproduces the reference's floats.  A cell whose stencil meets a list longer
-// than K is evaluated from the phi buffer over every grain instead.
+// reproduces the reference's floats while the step touches only the grains present
+// near each cell.  A cell whose stencil meets a list longer than K is evaluated
+// from the phi buffer over every grain instead.  dense_list_kernel builds the lists
+// of a buffer from scratch (one read of every grain) after the state is replaced
+// (init, set_slots, moving frame); while a buffer's lists are not valid the step
+// resets all of its grains.
 //
 // Boundary: set_BC_3D (PhaseField.cu:111-166) mirrors every face (halo 0 takes
 // cell 2, halo fn-1 takes cell fn-3) whatever the -b digits; the update reads
@@ -44,9 +49,13 @@ struct DenseArgs {
   const float4* orient;  // pack_orientations: entry g+1 is grain g
   const float* in;
   float* out;
-  const int* cnt;             // [len] list length (may exceed K)
+  const int* cnt;             // lists of `in`: [len] length (may exceed K)
   const unsigned short* lid;  // [K][len] grain of list entry
   const float* lval;          // [K][len] its phi
+  int* cnt_o;                 // lists of `out`: read for the reset, then rewritten
+  unsigned short* lid_o;
+  float* lval_o;
+  int reset_from_lists;       // 1: out's lists are valid (reset only the grains they name)
   unsigned long long* overflow;  // cells evaluated over every grain this step
 };
 
@@ -135,8 +144,6 @@ __global__ void __launch_bounds__(128) dense_update_kernel(const DenseArgs a) {
   nb[5] = i + (long long)a.fnx * mirror(j + 1, a.fny) + plane * k;
   nb[6] = i + (long long)a.fnx * j + plane * mirror(k + 1, a.fnz);
 
-  for (int g = 0; g < a.np; ++g) a.out[g * a.len + C] = -1.0f;
-
   const KineConst kc = kine_const(a.kin_delta);
   const float Up = dense_up(a, k);
   int c7[7];
@@ -146,6 +153,28 @@ __global__ void __launch_bounds__(128) dense_update_kernel(const DenseArgs a) {
     c7[s] = __ldg(a.cnt + nb[s]);
     over = over || c7[s] > a.K;
   }
+
+  // the output's grains that are not -1 (its content of two steps ago) back to -1
+  {
+    const int co = a.reset_from_lists ? a.cnt_o[C] : a.K + 1;
+    if (over || co > a.K) {
+      if (!over)
+        for (int g = 0; g < a.np; ++g) a.out[g * a.len + C] = -1.0f;
+    } else {
+      for (int e = 0; e < co; ++e) a.out[(long long)a.lid_o[e * a.len + C] * a.len + C] = -1.0f;
+    }
+  }
+
+  int cn = 0;  // the output's new list at C
+  auto emit = [&](int g, float v) {
+    if (v != -1.0f) {
+      if (cn < a.K) {
+        a.lid_o[cn * a.len + C] = (unsigned short)g;
+        a.lval_o[cn * a.len + C] = v;
+      }
+      ++cn;
+    }
+  };
 
   if (!over) {
     // centre list in registers (the repulsion sums run over it for every grain)
@@ -190,27 +219,33 @@ __global__ void __launch_bounds__(128) dense_update_kernel(const DenseArgs a) {
         if (e >= c7[3]) break;
         if (cid[e] != g) repul = repul_add(repul, cval[e]);
       }
-      a.out[g * a.len + C] = dense_grain(a, kc, g, v7, repul, Up);
+      const float v = dense_grain(a, kc, g, v7, repul, Up);
+      a.out[g * a.len + C] = v;
+      emit(g, v);
     }
-    return;
-  }
-
-  // a list past capacity somewhere in the stencil: every grain from the buffer
-  atomicAdd(a.overflow, 1ull);
-  for (int g = 0; g < a.np; ++g) {
-    float v7[7];
-    bool any = false;
+  } else {
+    // a list past capacity somewhere in the stencil: every grain from the buffer
+    atomicAdd(a.overflow, 1ull);
+    for (int g = 0; g < a.np; ++g) {
+      float v7[7];
+      bool any = false;
 #pragma unroll
-    for (int s = 0; s < 7; ++s) {
-      v7[s] = __ldg(a.in + g * a.len + nb[s]);
-      any = any || v7[s] != -1.0f;
+      for (int s = 0; s < 7; ++s) {
+        v7[s] = __ldg(a.in + g * a.len + nb[s]);
+        any = any || v7[s] != -1.0f;
+      }
+      float v = -1.0f;
+      if (any) {
+        float repul = 0.0f;
+        for (int q = 0; q < a.np; ++q)
+          if (q != g) repul = repul_add(repul, __ldg(a.in + q * a.len + C));
+        v = dense_grain(a, kc, g, v7, repul, Up);
+      }
+      a.out[g * a.len + C] = v;
+      emit(g, v);
     }
-    if (!any) continue;
-    float repul = 0.0f;
-    for (int q = 0; q < a.np; ++q)
-      if (q != g) repul = repul_add(repul, __ldg(a.in + q * a.len + C));
-    a.out[g * a.len + C] = dense_grain(a, kc, g, v7, repul, Up);
   }
+  a.cnt_o[C] = cn;
 }
 
 // set_minus1 x2 + ini_PF x2 (PhaseField.cu:51-57, 91-107): every grain -1, then

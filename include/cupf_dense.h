@@ -16,8 +16,10 @@
  * the repulsion sum over every other grain.  A grain whose phi is exactly -1 at
  * all seven stencil points stays exactly -1 and adds exactly zero to every
  * repulsion sum, so the library evaluates only the grains that differ from -1
- * somewhere in a cell's stencil (per-cell lists, see cupf_dense_set_tuning) and
- * writes -1 for the rest: the same floats as evaluating all of them.
+ * somewhere in a cell's stencil (per-cell lists of those grains, which each step
+ * writes for the next, see cupf_dense_set_tuning) and leaves the others at -1:
+ * the same floats as evaluating all of them, with traffic proportional to the
+ * grains present near each cell rather than to the number of grains.
  *
  * Status codes, precision and parameter structs are those of cupf.h.  All calls
  * on one handle are ordered on the handle's CUDA stream; handles are independent.

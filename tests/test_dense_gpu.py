@@ -260,6 +260,25 @@ def test_list_overflow_path_gives_the_same_bits(built):
         assert np.array_equal(a.get_slots(), b.get_slots())
 
 
+def test_carried_lists_equal_rebuilt_lists(built):
+    # the lists each step writes for the next, and lists rebuilt from the state
+    # (after set_slots), drive the same arithmetic; a capacity change mid-run too
+    c = _case(grains=8, seed=5)
+    ph = _developed(c, steps=20)
+    with DenseSolver(c) as a, DenseSolver(c) as b:
+        a.set_slots(ph, steps_done=20)
+        a.step(12)
+        mid = a.get_slots()
+        b.set_slots(mid, steps_done=32)
+        a.step(9)
+        b.step(4)
+        b.set_tuning(3)
+        b.step(2)
+        b.set_tuning(16)
+        b.step(3)
+        assert np.array_equal(a.get_slots(), b.get_slots())
+
+
 def test_matches_oracle_over_many_steps(built):
     c = _case(grains=8, seed=4)
     o = DenseOracle()
