@@ -300,17 +300,40 @@ static void set_zc(cupf_apt_handle* h, int zc) {
   h->nzc = (nz + h->zc - 1) / h->zc;
 }
 
-// Default z-chunk of a work item: 16 planes (the best of 8..128 on the
-// 256x256x512 NUM_PF=8 line case), halved to 8 when that leaves fewer than
-// about eight items per resident CTA (two per SM), so that the heavy-first
-// schedule still has items to balance.
+// Resident CTAs per SM the step kernel is compiled for (step_min_blocks).
+static int resident_per_sm(const cupf_apt_handle* h) {
+  int r = 2;
+  with_storage(h->prec, [&](auto tag) -> cupf_status {
+    using S = decltype(tag);
+    switch (h->g.np) {
+#define CASE(N)                          \
+  case N:                                \
+    r = step_min_blocks<N, S>();         \
+    break;
+      CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8)
+#undef CASE
+      default: break;
+    }
+    return CUPF_OK;
+  });
+  return r;
+}
+
+// Default z-chunk of a work item: the largest of 16, 8, 4, 2, 1 planes that
+// still gives at least 2.5 work items per resident CTA, else 1.  Measured on
+// the line case (B200, NUM_PF = 5 and 8): 16 is best from 128x128x256 up, while
+// 96^3 wants 4 and 64^3 or 48^3 want 1-2 (2.5-3x faster than 8 there) -- with
+// fewer items than CTAs most of the GPU idles, with many short items each pays
+// the two extra planes of its TMA pipeline fill.
 static int default_zc(cupf_apt_handle* h) {
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
   const long long tiles = (long long)((h->p.fnx - 2 + TX - 1) / TX) * ((h->p.fny - 2 + TY - 1) / TY);
   const int nz = h->p.fnz - 2;
-  if (tiles * ((nz + 15) / 16) < 8LL * 2 * nsm) return 8;
-  return 16;
+  const long long want = (5LL * resident_per_sm(h) * nsm + 1) / 2;
+  for (int zc = 16; zc > 1; zc /= 2)
+    if (tiles * ((nz + zc - 1) / zc) >= want) return zc;
+  return 1;
 }
 
 static int grid_for(long long n, int block = 256) {
