@@ -50,6 +50,13 @@ struct StepSmem {
   static constexpr int kBytes = kBarOff + STAGES * 8 + 16;  // + abort word, issued count
 };
 
+// Per-slot update loop shape of a storage format: rolled for the 16-bit pairs,
+// unrolled over NUM_PF for FP32 (each measured faster for its format).
+template <class S>
+struct RolledSlots {
+  static constexpr bool value = S::kBytes == 4;
+};
+
 template <int NP>
 using CodeMap = typename std::conditional<(NP <= 8), uint32_t, unsigned long long>::type;
 
@@ -413,48 +420,61 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
       Up = __fdiv_rn(T, a.L_cp);
     }
 
+    // New value of output slot j < n holding grain `id`.
+    auto update_slot = [&](int j, int id) -> P {
+      // orientation of the grain (APTPhaseField.cu:259-273): loads issued before
+      // the stencil values are gathered so their latency overlaps; ids are >= 0
+      // here (cupf_apt_set_slots rejects other negative ids) and the clamp only
+      // keeps a corrupted id from reading outside the tables
+      int tid2 = id;
+      if (id > a.num_theta) tid2 = (id % a.num_theta) + 1;
+      const bool tab_ok = (unsigned)tid2 <= (unsigned)a.num_theta;
+      const int ti = tab_ok ? tid2 : 0;
+      const float4 t_o = __ldg(a.orient + ti);  // {sint[ti], cost[ti], sint[ti+NG], cost[ti+NG]}
+      float ph7[7];
 #pragma unroll
-    for (int j = 0; j < NP; ++j) {
-      P o;
-      if (j >= n) {
-        o = S::empty();
-      } else if (!upd) {
-        o = outp[j * ss];  // reference leaves the slot unwritten
-      } else {
-        const int id = L[j];
-        // orientation of the grain (APTPhaseField.cu:259-273): loads issued before
-        // the stencil values are gathered so their latency overlaps; ids are >= 0
-        // here (cupf_apt_set_slots rejects other negative ids) and the clamp only
-        // keeps a corrupted id from reading outside the tables
-        int tid2 = id;
-        if (id > a.num_theta) tid2 = (id % a.num_theta) + 1;
-        const bool tab_ok = (unsigned)tid2 <= (unsigned)a.num_theta;
-        const int ti = tab_ok ? tid2 : 0;
-        const float4 t_o = __ldg(a.orient + ti);  // {sint[ti], cost[ti], sint[ti+NG], cost[ti+NG]}
-        float ph7[7];
-#pragma unroll
-        for (int s = 0; s < 7; ++s) ph7[s] = fetch(s, j);
-        float sina = 0.0f, cosa = 1.0f, sinb = 0.0f, cosb = 1.0f;
-        if (ph7[3] > kLS && tab_ok) {  // (double)phC > LS
-          sina = t_o.x;
-          cosa = t_o.y;
-          sinb = t_o.z;
-          cosb = t_o.w;
-        }
-        float repul = 0.0f;
-#pragma unroll
-        for (int q = 0; q < NP; ++q) {
-          if (q >= n) break;
-          if (q != j) repul = repul_add(repul, phc[q]);
-        }
-        const float nv = slot_update(a, kc, ph7, sina, cosa, sinb, cosb, repul, Up);
-        const int oid = (nv < kDrop) ? -1 : id;  // (double)nv < -0.9999
-        if (S::kStochastic)
-          o = S::make_sr(nv, oid, mix32(cell_key + (uint32_t)j * 0x9E3779B9u));
-        else
-          o = S::make(nv, oid);
+      for (int s = 0; s < 7; ++s) ph7[s] = fetch(s, j);
+      float sina = 0.0f, cosa = 1.0f, sinb = 0.0f, cosb = 1.0f;
+      if (ph7[3] > kLS && tab_ok) {  // (double)phC > LS
+        sina = t_o.x;
+        cosa = t_o.y;
+        sinb = t_o.z;
+        cosb = t_o.w;
       }
-      outp[j * ss] = o;
+      float repul = 0.0f;
+#pragma unroll
+      for (int q = 0; q < NP; ++q) {
+        if (q >= n) break;
+        if (q != j) repul = repul_add(repul, phc[q]);
+      }
+      const float nv = slot_update(a, kc, ph7, sina, cosa, sinb, cosb, repul, Up);
+      const int oid = (nv < kDrop) ? -1 : id;  // (double)nv < -0.9999
+      if (S::kStochastic) return S::make_sr(nv, oid, mix32(cell_key + (uint32_t)j * 0x9E3779B9u));
+      return S::make(nv, oid);
+    };
+    if (RolledSlots<S>::value) {
+      // 16-bit pairs: one loop body run to the cell's slot count (the smaller code
+      // and register footprint measured faster at three CTAs per SM)
+#pragma unroll
+      for (int j = 0; j < NP; ++j)
+        if (j >= n) outp[j * ss] = S::empty();
+      if (upd) {
+#pragma unroll 1
+        for (int j = 0; j < n; ++j) {
+          int id = L[0];
+#pragma unroll
+          for (int q = 1; q < NP; ++q) id = (j == q) ? L[q] : id;
+          outp[j * ss] = update_slot(j, id);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < NP; ++j) {
+        if (j >= n)
+          outp[j * ss] = S::empty();
+        else if (upd)  // else the reference leaves the slot unwritten
+          outp[j * ss] = update_slot(j, L[j]);
+      }
     }
   }
 
