@@ -60,6 +60,46 @@ def test_c1_200_steps_bit_exact(built):
     assert (n_id, n_ph) == (0, 0), (n_id, n_ph, d)
 
 
+def test_c2_200_steps_bit_exact(built):
+    """Configuration C2 (the benchmark workload): 256x256x512 interior, 600 grains,
+    NUM_PF=8, its parity window of 200 steps; then the argmax map of both."""
+    import torch
+    from cupf_b200.solver import APTSolver
+    from oracle import RefGPU
+    from tests.helpers import face_mask
+    c = cases.line_case(256, 256, 512, num_pf=8, num_grains=600, seed=0, bc="110")
+    p = c.params
+    ref_ph, ref_id = run_reference_gpu(c, 200)
+    my_ph, my_id = run_cupf(c, 200)
+    m = face_mask(p)
+    L = c.length
+    n_id = n_ph = 0
+    for q in range(p.num_pf):  # slot by slot (each slot is 137 MB per array)
+        sl = slice(q * L, (q + 1) * L)
+        n_id += int(np.count_nonzero(my_id[sl][m] != ref_id[sl][m]))
+        n_ph += int(np.count_nonzero(my_ph[sl][m].view(np.int32) != ref_ph[sl][m].view(np.int32)))
+    assert (n_id, n_ph) == (0, 0), (n_id, n_ph)
+    ref = RefGPU(8)
+    ref.check(ref.L.ref_set_params(p))
+    d_ph = torch.from_numpy(ref_ph).cuda()
+    d_id = torch.from_numpy(ref_id).cuda()
+    del ref_ph, ref_id, my_ph, my_id
+    phi = torch.zeros(L, dtype=torch.float32, device="cuda")
+    alpha = torch.zeros(L, dtype=torch.int32, device="cuda")
+    ref.check(ref.L.ref_collect(d_ph.data_ptr(), phi.data_ptr(), alpha.data_ptr(), d_id.data_ptr()))
+    torch.cuda.synchronize()
+    r_phi, r_alpha = phi.cpu().numpy(), alpha.cpu().numpy()
+    del d_ph, d_id, phi, alpha
+    torch.cuda.empty_cache()
+    ph0, id0 = c.initial_slots()
+    with APTSolver(c) as s:
+        s.set_slots(ph0, id0, 0)
+        s.step(200)
+        my_phi, my_alpha = s.collect(clear=True)
+    assert np.array_equal(my_alpha[m], r_alpha[m])
+    assert np.array_equal(my_phi[m].view(np.int32), r_phi[m].view(np.int32))
+
+
 def test_collect_matches_reference(built):
     import torch
     from oracle import RefGPU
