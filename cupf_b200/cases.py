@@ -226,3 +226,58 @@ def line_case(nx_int: int, ny_int: int, nz_int: int, num_pf: int = 5, num_grains
                 phi=phi.reshape(-1), alpha=alpha.reshape(-1),
                 meta=dict(kind="line", interior=(nx_int, ny_int, nz_int), num_grains=num_grains,
                           seed=seed, G=G, R=R, bc=bc))
+
+
+def cone_case(nx_int: int, ny_int: int, nz_int: int, num_pf: int = 5, num_grains: int = 20,
+              seed: int = 0, angle: float = 1.0, V: float = 0.2, bc: str = "110", **kw) -> Case:
+    """The line case's grains and initial field under the cone undercooling of
+    thermalType 3 (APTPhaseField.cu:292-307): dist = cos(angle) * (sqrt((y -
+    lyd/2)^2 + (z0 + lzd - z)^2) - r0(x)), r0(x) = z0 + (r0 - z0) x / lm, lm =
+    (r0 - z0) / tan(angle), T = -G dist - UC 1e6 t; cells with x > lm + V 1e6 t
+    are not updated.  angle in rad, V in m/s."""
+    c = line_case(nx_int, ny_int, nz_int, num_pf, num_grains, seed, bc=bc, **kw)
+    p = c.params
+    p.thermalType = 3
+    p.angle = F32(angle)
+    p.V = F32(V)
+    c.meta.update(kind="cone", angle=angle, V=V)
+    return c
+
+
+def paraboloid_case(nx_int: int, ny_int: int, nz_int: int, num_pf: int = 5, num_grains: int = 20,
+                    seed: int = 0, V: float = 0.5, mp_frac: float = 0.75, curvature: float = 0.15,
+                    order: float = 1.0, bc: str = "110", **kw) -> Case:
+    """The line case's grains and initial field under the table undercooling of
+    thermalType 4 (APTPhaseField.cu:308-325, interp3Dtemperature
+    devicefunc.cu_inl:85-125): T = -G * psi(x - V 1e6 t, y, z) (order != 100)
+    interpolated trilinearly from a table on a grid of spacing 2 dx W0, with psi a
+    paraboloid melt-pool distance psi = z0 - z + curvature * ((x - xc)^2 + (y -
+    yc)^2) / lz.  Cells whose shifted x leaves [0, mp_len + x0] are not updated;
+    mp_len = mp_frac * lxd, x0 = 0.  The table covers every query the interior
+    can make (the reference does not bound its index), with two spare points."""
+    c = line_case(nx_int, ny_int, nz_int, num_pf, num_grains, seed, bc=bc, **kw)
+    p = c.params
+    dxd = F32(F32(p.dx) * F32(p.W0))
+    lxd = F32((p.fnx - 3) * dxd)
+    p.thermalType = 4
+    p.V = F32(V)
+    p.x0 = F32(0)
+    p.mp_len = F32(F32(mp_frac) * lxd)
+    p.order = F32(order)
+    D = float(F32(2 * dxd))
+    nx = int(math.ceil((float(p.mp_len) + float(p.x0)) / D)) + 3
+    ny = int(math.ceil((float(p.lyd) + 4 * float(dxd)) / D)) + 3
+    nz = int(math.ceil((float(p.lzd) + 4 * float(dxd)) / D)) + 3
+    X = (np.arange(nx) * D).astype(F32)
+    Y = (-2 * float(dxd) + np.arange(ny) * D).astype(F32)
+    Z = (-2 * float(dxd) + np.arange(nz) * D).astype(F32)
+    xc, yc = 0.5 * float(p.mp_len), 0.5 * float(p.lyd)
+    lz = float(p.lzd)
+    zz, yy, xx = np.meshgrid(Z.astype(np.float64), Y.astype(np.float64), X.astype(np.float64),
+                             indexing="ij")
+    psi = float(p.z0) - zz + curvature * ((xx - xc) ** 2 + (yy - yc) ** 2) / lz
+    p.Nx, p.Ny, p.Nz = nx, ny, nz
+    c.X_mac, c.Y_mac, c.Z_mac = X, Y, Z
+    c.psi_mac = psi.astype(F32).reshape(-1)  # x fastest (index kx + ky*Nx + kz*Nx*Ny)
+    c.meta.update(kind="paraboloid", V=V, mp_len=float(p.mp_len), curvature=curvature, order=order)
+    return c

@@ -122,9 +122,15 @@ __device__ __forceinline__ float interp3d(const float* __restrict__ u, float x, 
   long long on = kx + (long long)ky * Nx + (long long)(kz + 1) * Nx * Ny;
   float a = fmul(fsub(1.0f, dx), fsub(1.0f, dy)), b = fmul(fsub(1.0f, dx), dy);
   float c = fmul(dx, fsub(1.0f, dy)), d = fmul(dx, dy);
-  float p0 = ffma(c, __ldg(u + o + 1), ffma(a, __ldg(u + o), fmul(b, __ldg(u + o + Nx))));
+  // the reference's build fuses the first pair of the two brackets on opposite
+  // sides (pinned on dumps of the paraboloid case): lower a*u0 + b*u1 fuses the
+  // right product, upper the left one; the rest of each sum and the z blend fuse
+  // as written left to right
+  float p0 = ffma(b, __ldg(u + o + Nx), fmul(a, __ldg(u + o)));
+  p0 = ffma(c, __ldg(u + o + 1), p0);
   p0 = ffma(d, __ldg(u + o + Nx + 1), p0);
-  float p1 = ffma(c, __ldg(u + on + 1), ffma(a, __ldg(u + on), fmul(b, __ldg(u + on + Nx))));
+  float p1 = ffma(a, __ldg(u + on), fmul(b, __ldg(u + on + Nx)));
+  p1 = ffma(c, __ldg(u + on + 1), p1);
   p1 = ffma(d, __ldg(u + on + Nx + 1), p1);
   return ffma(p0, fsub(1.0f, dz), fmul(p1, dz));
 }
@@ -160,7 +166,7 @@ __device__ __forceinline__ bool tinterp(const StepArgs& a, int i, int j, int k, 
     float r0x = fadd(a.z0, __fdiv_rn(fmul(fsub(a.r0, a.z0), xl), lm));
     float u = fsub(__ldg(a.y + j), fmul(0.5f, a.lyd));
     float zt = fsub(fadd(a.z0, a.lzd), __ldg(a.z + k));
-    float dist = fmul(cosf(a.angle), fsub(__fsqrt_rn(ffma(u, u, fmul(zt, zt))), r0x));
+    float dist = fmul(cosf(a.angle), fsub(__fsqrt_rn(ffma(zt, zt, fmul(u, u))), r0x));
     if ((double)xl > __fma_rn((double)fmul(a.V, t), 1e6, (double)lm)) return false;
     double m = __dmul_rn((double)a.uc, 1e6);
     *T = __double2float_rn(__fma_rn(-m, (double)t, (double)fmul(-a.G, dist)));

@@ -69,10 +69,24 @@ enum {
   S_RHS,     /* E1 - (lamd*Up)*inner                    : 0/1 */
   S_NEW,     /* phC + dt*dphi                           : 0/1 */
   S_TD,      /* (double)a - (UC*1e6)*t in double        : 0/1 */
+  /* thermalType 3 (cone) and 4 (paraboloid table) */
+  S_T3_YU,   /* y - 0.5*lyd                             : 0/1 */
+  S_T3_SQ,   /* u*u + zt*zt                             : 0/1/2 */
+  S_T3_SKIP, /* lm + (V*t)*1e6 in double                : 0/1 */
+  S_T3_TD,   /* (double)(-G*dist) - (UC*1e6)*t          : 0/1 */
+  S_T4_XQ,   /* (double)x - (V*t)*1e6                   : 0/1 */
+  S_T4_P1,   /* a*u0 + b*u1 (trilinear corner weights)  : 0/1/2 */
+  S_T4_P2,   /* + c*u2                                  : 0/1 */
+  S_T4_P3,   /* + d*u3                                  : 0/1 */
+  S_T4_Z,    /* p0*(1-dz) + p1*dz                       : 0/1/2 */
+  S_T4_Q1,   /* the upper bracket's a*u0 + b*u1         : 0/1/2 */
+  S_T4_Q2,   /* + c*u2                                  : 0/1 */
+  S_T4_Q3,   /* + d*u3                                  : 0/1 */
   S_NSITES
 };
 
-static int g_cfg[S_NSITES] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
+static int g_cfg[S_NSITES] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1,
+                              0, 1, 1, 1, 0, 1, 1, 1, 1, 1, 1, 1};
 
 int oracle_num_sites(void) { return S_NSITES; }
 
@@ -177,11 +191,13 @@ static float interp3d_f32(const float* u, float x, float y, float z, int Nx, int
   int64_t o = kx + (int64_t)ky * Nx + (int64_t)kz * Nx * Ny;
   int64_t on = kx + (int64_t)ky * Nx + (int64_t)(kz + 1) * Nx * Ny;
   float a = (1.0f - dx) * (1.0f - dy), b = (1.0f - dx) * dy, c = dx * (1.0f - dy), d = dx * dy;
-  float p0 = fmaf(c, u[o + 1], fmaf(a, u[o], b * u[o + Nx]));
-  p0 = fmaf(d, u[o + Nx + 1], p0);
-  float p1 = fmaf(c, u[on + 1], fmaf(a, u[on], b * u[on + Nx]));
-  p1 = fmaf(d, u[on + Nx + 1], p1);
-  return fmaf(p0, 1.0f - dz, p1 * dz);
+  float p0 = sop(a, u[o], b, u[o + Nx], g_cfg[S_T4_P1]);
+  p0 = g_cfg[S_T4_P2] ? fmaf(c, u[o + 1], p0) : p0 + c * u[o + 1];
+  p0 = g_cfg[S_T4_P3] ? fmaf(d, u[o + Nx + 1], p0) : p0 + d * u[o + Nx + 1];
+  float p1 = sop(a, u[on], b, u[on + Nx], g_cfg[S_T4_Q1]);
+  p1 = g_cfg[S_T4_Q2] ? fmaf(c, u[on + 1], p1) : p1 + c * u[on + 1];
+  p1 = g_cfg[S_T4_Q3] ? fmaf(d, u[on + Nx + 1], p1) : p1 + d * u[on + Nx + 1];
+  return sop(p0, 1.0f - dz, p1, dz, g_cfg[S_T4_Z]);
 }
 
 /* Thermal undercooling at (i,j,k,t); returns 0 when the reference `continue`s
@@ -207,14 +223,17 @@ static int tinterp_f32(const cupf_apt_params* p, const cupf_apt_inputs* th, int 
     float lm = (p->r0 - p->z0) / tanf(p->angle);
     float xl = th->x[i] - 0.0f;
     float r0x = p->z0 + (p->r0 - p->z0) * xl / lm;
-    float a = th->y[j] - 0.5f * p->lyd;
+    float a = g_cfg[S_T3_YU] ? fmaf(-0.5f, p->lyd, th->y[j]) : th->y[j] - 0.5f * p->lyd;
     float zt = p->z0 + p->lzd - th->z[k];
-    float dist = cosf(p->angle) * (sqrtf(fmaf(a, a, zt * zt)) - r0x);
-    if ((double)xl > fma((double)(p->V * t), 1e6, (double)lm)) return 0;
+    float dist = cosf(p->angle) * (sqrtf(sop(a, a, zt, zt, g_cfg[S_T3_SQ])) - r0x);
+    double vt = (double)(p->V * t);
+    if ((double)xl > (g_cfg[S_T3_SKIP] ? fma(vt, 1e6, (double)lm) : (double)lm + vt * 1e6)) return 0;
     double m = (double)p->underCoolingRate * 1e6;
-    T = (float)fma(-m, (double)t, (double)(-p->G * dist));
+    double gd = (double)(-p->G * dist);
+    T = (float)(g_cfg[S_T3_TD] ? fma(-m, (double)t, gd) : gd - m * (double)t);
   } else if (p->thermalType == 4) {
-    float xq = (float)((double)th->x[i] - (double)(p->V * t) * 1e6);
+    double vt = (double)(p->V * t);
+    float xq = (float)(g_cfg[S_T4_XQ] ? fma(-vt, 1e6, (double)th->x[i]) : (double)th->x[i] - vt * 1e6);
     if (xq > p->mp_len + p->x0 || xq < 0.0f) return 0;
     float Dx = th->X_mac[1] - th->X_mac[0];
     float v = interp3d_f32(th->psi_mac, xq - th->X_mac[0], th->y[j] - th->Y_mac[0],

@@ -7,7 +7,7 @@ one padding row on the merge's local array) on seeded synthetic cases and writes
 their states as compressed .npz files.  The CPU tests pin the oracle against
 these files bit-for-bit.
 
-Usage:  python tests/golden/make_golden.py OUT_DIR
+Usage:  python tests/golden/make_golden.py OUT_DIR [CASE ...]
 """
 import os
 import sys
@@ -29,6 +29,8 @@ CASES = {
     "g3_np5_111_iuc": ((24, 24, 24), 5, 40, 2, "111", [0, 1, 10, 11], {"iuc": True}),
     "g4_np5_cyl": ((24, 24, 32), 5, 20, 3, "110", [0, 1, 12, 13], {"thermal": 2}),
     "c1_64_np5": ((64, 64, 64), 5, 20, 0, "110", [0, 200], {"final_only": True}),
+    "g5_np5_cone": ((40, 24, 32), 5, 20, 10, "110", [0, 1, 12, 13], {"thermal": 3}),
+    "g6_np8_parab": ((36, 28, 32), 8, 30, 11, "110", [0, 1, 12, 13], {"thermal": 4}),
 }
 
 
@@ -42,7 +44,8 @@ def ptr(t):
 
 def run_case(name, spec, out_dir):
     interior, num_pf, grains, seed, bc, saves, opt = spec
-    c = cases.line_case(*interior, num_pf=num_pf, num_grains=grains, seed=seed, bc=bc)
+    build = {3: cases.cone_case, 4: cases.paraboloid_case}.get(opt.get("thermal"), cases.line_case)
+    c = build(*interior, num_pf=num_pf, num_grains=grains, seed=seed, bc=bc)
     p = c.params
     if opt.get("thermal") == 2:
         p.thermalType = 2
@@ -53,6 +56,9 @@ def run_case(name, spec, out_dir):
     ref.check(ref.L.ref_set_params(p))
     ph0, id0 = c.initial_slots()
     x, y, z, sint, cost = (dev(a) for a in (c.x, c.y, c.z, c.sint, c.cost))
+    # macro tables of thermalType 4 (None: the harness passes a zeroed buffer)
+    mac = [getattr(c, n, None) for n in ("X_mac", "Y_mac", "Z_mac", "t_mac", "psi_mac", "T_3D")]
+    mac = [dev(np.asarray(m, np.float32)) if m is not None else None for m in mac]
     a_ph, a_id = dev(ph0), dev(id0)
     b_ph, b_id = dev(ph0), dev(id0)
     rec = {}
@@ -63,8 +69,8 @@ def run_case(name, spec, out_dir):
         t = np.float32(np.float32(n) * np.float32(p.dt)) * np.float32(p.tau0)
         ref.check(ref.L.ref_set_bc(ptr(a_ph), ptr(a_id)))
         ref.check(ref.L.ref_rhs_psi(float(t), ptr(x), ptr(y), ptr(z), ptr(a_ph), ptr(b_ph),
-                                    ptr(a_id), ptr(b_id), ptr(sint), ptr(cost), None, None, None,
-                                    None, None, None, int(iuc)))
+                                    ptr(a_id), ptr(b_id), ptr(sint), ptr(cost),
+                                    *(ptr(m) for m in mac), int(iuc)))
         a_ph, b_ph = b_ph, a_ph
         a_id, b_id = b_id, a_id
         if n in saves:
@@ -120,8 +126,10 @@ def run_case(name, spec, out_dir):
 def main():
     out_dir = sys.argv[1] if len(sys.argv) > 1 else os.path.dirname(os.path.abspath(__file__))
     os.makedirs(out_dir, exist_ok=True)
+    only = set(sys.argv[2:])
     for name, spec in CASES.items():
-        run_case(name, spec, out_dir)
+        if not only or name in only:
+            run_case(name, spec, out_dir)
 
 
 if __name__ == "__main__":

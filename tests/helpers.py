@@ -49,14 +49,18 @@ def run_reference_gpu(case, nsteps, use_iuc=False, ph0=None, id0=None):
         ph0, id0 = case.initial_slots()
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
     x, y, z, sint, cost = (dev(a) for a in (case.x, case.y, case.z, case.sint, case.cost))
+    # macro tables of thermalType 4 (the harness substitutes a zeroed buffer for None)
+    mac = [getattr(case, n, None) for n in ("X_mac", "Y_mac", "Z_mac", "t_mac", "psi_mac", "T_3D")]
+    mac_d = [dev(np.asarray(m, np.float32)) if m is not None else None for m in mac]
+    mac_p = [m.data_ptr() if m is not None else None for m in mac_d]
     a_ph, a_id, b_ph, b_id = dev(ph0), dev(id0), dev(ph0), dev(id0)
     for n in range(1, nsteps + 1):
         t = np.float32(np.float32(n) * np.float32(p.dt)) * np.float32(p.tau0)
         ref.check(ref.L.ref_set_bc(a_ph.data_ptr(), a_id.data_ptr()))
         ref.check(ref.L.ref_rhs_psi(float(t), x.data_ptr(), y.data_ptr(), z.data_ptr(),
                                     a_ph.data_ptr(), b_ph.data_ptr(), a_id.data_ptr(),
-                                    b_id.data_ptr(), sint.data_ptr(), cost.data_ptr(), None, None,
-                                    None, None, None, None, int(use_iuc)))
+                                    b_id.data_ptr(), sint.data_ptr(), cost.data_ptr(), *mac_p,
+                                    int(use_iuc)))
         a_ph, b_ph = b_ph, a_ph
         a_id, b_id = b_id, a_id
     ref.check(ref.L.ref_set_bc(a_ph.data_ptr(), a_id.data_ptr()))

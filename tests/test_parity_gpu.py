@@ -27,11 +27,20 @@ SMALL = [
     ((40, 40, 48), 8, 90, 7, "110", 60, False, 1),
     ((16, 16, 20), 2, 5, 8, "000", 15, False, 1),
     ((20, 20, 20), 1, 3, 9, "110", 10, False, 1),
+    ((40, 24, 32), 5, 20, 10, "110", 20, False, 3),  # cone: cells past the cone front skipped
+    ((36, 28, 32), 8, 30, 11, "110", 20, False, 4),  # paraboloid table, trilinear lookups
+    ((48, 20, 40), 6, 25, 12, "111", 40, False, 4),
+    ((30, 30, 36), 4, 12, 13, "110", 40, False, 3),
 ]
 
 
 def _case(spec):
     interior, npf, grains, seed, bc, steps, iuc, thermal = spec
+    if thermal == 3:
+        return cases.cone_case(*interior, num_pf=npf, num_grains=grains, seed=seed, bc=bc), steps, iuc
+    if thermal == 4:
+        return (cases.paraboloid_case(*interior, num_pf=npf, num_grains=grains, seed=seed, bc=bc),
+                steps, iuc)
     c = cases.line_case(*interior, num_pf=npf, num_grains=grains, seed=seed, bc=bc)
     if thermal == 2:
         c.params.thermalType = 2
