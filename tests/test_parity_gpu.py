@@ -31,6 +31,7 @@ SMALL = [
     ((36, 28, 32), 8, 30, 11, "110", 20, False, 4),  # paraboloid table, trilinear lookups
     ((48, 20, 40), 6, 25, 12, "111", 40, False, 4),
     ((30, 30, 36), 4, 12, 13, "110", 40, False, 3),
+    ((24, 24, 24), 5, 10, 14, "110", 15, False, 0),  # no thermal model: Tinterp = 0
 ]
 
 
@@ -42,6 +43,8 @@ def _case(spec):
         return (cases.paraboloid_case(*interior, num_pf=npf, num_grains=grains, seed=seed, bc=bc),
                 steps, iuc)
     c = cases.line_case(*interior, num_pf=npf, num_grains=grains, seed=seed, bc=bc)
+    if thermal == 0:
+        c.params.thermalType = 0
     if thermal == 2:
         c.params.thermalType = 2
         c.params.r0 = np.float32(0.5) * c.params.lzd
