@@ -178,7 +178,7 @@ cupf_status cupf_apt_grain_volumes(cupf_apt_handle* h, int32_t num_grains,
  *   out[1] = sum |grad m|/2         interface area in cell faces (central differences)
  *   out[2] = out[0] / (interior cells per layer)   mean interface height in cells
  * Reduced in double in a fixed order (deterministic).  Supplies the volume and
- * interface measures the split-precision error is judged on; the reference has
+ * interface measures the split-precision error is measured on; the reference has
  * no counterpart (its QoIs are integer voxel counts, QOI.cpp:38-231). */
 cupf_status cupf_apt_qoi_sums(cupf_apt_handle* h, double* out);
 

@@ -1,7 +1,7 @@
 """Device time of the reference step (APTsetBC3D + APTrhs_psi as its evolve loop
 launches them, compiled for sm_100a) against the library's fused step, on the
 C2 throughput configuration (256x256x512 interior, 600 grains, NUM_PF=8).
-Records both in gpurun_out/perf_vs_reference.json and checks that the library
+Records both in perf_vs_reference.json (in $CUPF_RECORD_DIR) and checks that the library
 is faster.
 """
 import json
@@ -48,7 +48,7 @@ def test_step_faster_than_reference_c2(built):
            "reference_ms_per_step": ref_ms, "cupf_ms_per_step": my_ms,
            "reference_mcell_per_s": cells / ref_ms / 1e3, "cupf_mcell_per_s": cells / my_ms / 1e3,
            "speedup": ref_ms / my_ms}
-    out = os.path.join(os.path.dirname(os.path.dirname(__file__)), "gpurun_out")
+    out = os.environ.get("CUPF_RECORD_DIR", "")
     if os.path.isdir(out):
         with open(os.path.join(out, "perf_vs_reference.json"), "w") as f:
             json.dump(rec, f, indent=1)

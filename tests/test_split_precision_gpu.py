@@ -7,8 +7,8 @@ BF16 storage on the GPU and in FP64 on the CPU (the oracle).  Compared:
     as the volume-weighted L1 relative error sum|V_g - V64_g| / sum V64_g;
   * the mean interface height (FP64 solid volume / base area);
   * the FP64 interface area.
-Tolerance (north_star): 1e-3 relative on volume fractions and interface position.
-The measured errors are written to gpurun_out/split_precision.json when that
+Tolerance: 1e-3 relative on volume fractions and interface position.
+The measured errors are written to $CUPF_RECORD_DIR/split_precision_*.json when that
 directory exists.
 """
 import json
@@ -59,7 +59,7 @@ def test_split_precision_error(built, fp64_reference, prec):
     rec = {"precision": prec, "steps": NSTEPS, "volume_fraction_l1_rel_err": vol_err,
            "interface_height_rel_err": pos_err, "interface_area_rel_err": area_err,
            "interface_height_cells": qs[2], "interface_height_fp64": q64[2]}
-    out = os.path.join(os.path.dirname(os.path.dirname(__file__)), "gpurun_out")
+    out = os.environ.get("CUPF_RECORD_DIR", "")
     if os.path.isdir(out):
         with open(os.path.join(out, "split_precision_%s.json" % prec), "w") as f:
             json.dump(rec, f)
