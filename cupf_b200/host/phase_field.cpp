@@ -554,18 +554,42 @@ bool APTPhaseField::moveDomain(MovingDomain* md) {
   return true;
 }
 
-// APTPhaseField::evolve (APTPhaseField.cu:710-946) without MPI and nucleation.
+// APTPhaseField::evolve (APTPhaseField.cu:710-946) without MPI.  With -n the
+// liquid-start phase (:779-816) runs first when preMt > 0: from an all-liquid
+// state, preMt steps at the liquid-start undercooling with a nucleation pass after
+// every odd step; the grains it grew then label the solid cells of the initial
+// phase field (APTini_PF from phi_old and the collected alpha, :820-822).  The
+// main loop nucleates after every odd step (:866-870).  The reference's update at
+// t = 0 on the freshly emptied state (:776) changes nothing and is not issued.
+// Without -n, preMt is ignored: the reference's liquid-start phase launches
+// add_nucl on the status and generator arrays that only -n allocates (:733-745).
 bool APTPhaseField::evolve() {
   const DesignSettingData* ds = GetSetDesignSetting();
-  if (ds->includeNucleation) return setErr("nucleation is not built in this driver");
+  const bool nucl = ds->includeNucleation;
   MovingDomain md;
+  if (nucl && params.preMt > 0) {
+    const std::vector<float> liquid((size_t)length, -1.0f);
+    if (!check(cupf_apt_init_from_argmax(mHandle, liquid.data(), alpha.data()), "init") ||
+        !check(cupf_apt_nucl_init(mHandle), "nucleation init") ||
+        !check(cupf_apt_nucl_reset(mHandle), "nucleation reset"))
+      return false;
+    for (int kt = 0; kt < params.preMt / 2; kt++) {
+      if (!check(cupf_apt_step(mHandle, 1, 1), "cupf_apt_step") ||
+          !check(cupf_apt_nucleate(mHandle, 1, nullptr), "cupf_apt_nucleate") ||
+          !check(cupf_apt_step(mHandle, 1, 1), "cupf_apt_step"))
+        return false;
+    }
+    if (!collectToHost(true)) return false;  // alpha_m of the grown grains
+  }
   if (!check(cupf_apt_init_from_argmax(mHandle, phi.data(), alpha.data()), "init")) return false;
+  if (nucl && params.preMt <= 0 && !check(cupf_apt_nucl_init(mHandle), "nucleation init"))
+    return false;
   if (!collectToHost(true)) return false;
   if (ds->useLineConfig) {
     md.allocateMovingDomain(params.num_theta, fnz);
     qois->calculateLineQoIs(qoiGrid(), md.cur_tip, alpha.data(), 0, z.data(),
                             md.loss_area_host.data(), md.move_count);
-  } else {
+  } else if (!nucl) {
     qois->calculateQoIs(qoiGrid(), alpha.data(), 0);
   }
   const int qoikts = params.Mt / params.nts;
@@ -575,6 +599,7 @@ bool APTPhaseField::evolve() {
   int kt = 0;
   for (kt = 0; kt < kt_max; kt++) {
     if (!check(cupf_apt_step(mHandle, 1, 0), "cupf_apt_step")) return false;
+    if (nucl && !check(cupf_apt_nucleate(mHandle, 0, nullptr), "cupf_apt_nucleate")) return false;
     if (ds->useLineConfig) {
       if (!getLineQoIs(&md)) return false;
       if (md.samples == params.nts) break;

@@ -20,8 +20,9 @@ INPUT_KEYS = ["Tmelt", "Dh", "L_cp", "GT", "beta0", "mu_k", "delta", "kin_delta"
 
 
 def write_input_file(path, Lx, nts=2, asp_ratio_yx=1.0, asp_ratio_zx=2.0, moving_ratio=1.0,
-                     macro=(13, 13, 23, 11), num_pf=8, extra=None):
-    """A line.py-style parameter file (`key = value` per line)."""
+                     macro=(13, 13, 23, 11), num_pf=8, extra=None, pre_mt=0):
+    """A line.py-style parameter file (`key = value` per line).  pre_mt is the
+    number of liquid-start steps a nucleation run takes first (preMt)."""
     vals = dict(LINE_CONSTANTS)
     if extra:
         vals.update(extra)
@@ -33,15 +34,20 @@ def write_input_file(path, Lx, nts=2, asp_ratio_yx=1.0, asp_ratio_zx=2.0, moving
               "nt = %d" % macro[3], "haloWidth = 1", "xmin = 0", "ymin = 0", "zmin = 0",
               "eta = 0.0", "noi_period = 200", "ictype = 0", "asp_ratio_yx = %r" % asp_ratio_yx,
               "asp_ratio_zx = %r" % asp_ratio_zx, "moving_ratio = %r" % moving_ratio,
-              "nts = %d" % nts, "Lx = %r" % Lx, "preMt = 0", "NUM_PF = %d" % num_pf]
+              "nts = %d" % nts, "Lx = %r" % Lx, "preMt = %d" % pre_mt, "NUM_PF = %d" % num_pf]
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
 
 
 def write_line_forcing(folder, Lx, Ly, Lz, num_grains, seed, G, R, z0, top, t_end,
-                       periodic=True, macro=(13, 13, 23, 11), dxd=0.08):
+                       periodic=True, macro=(13, 13, 23, 11), dxd=0.08, nmax=0.01,
+                       cooling_rate=None):
     """The forcing folder of a line run: macro grid, psi = z0 - z, substrate ids
-    (alpha.txt, (nx+1)x(ny+1) values), orientations, scalars."""
+    (alpha.txt, (nx+1)x(ny+1) values), orientations, scalars.  nmax is the
+    nucleation density (Nmax.txt).  With cooling_rate (K/s) the folder also holds
+    the 4-D temperature table Temp.txt (the reference's Temp.h5:/Temp, x fastest,
+    t slowest) of a uniform melt cooling from the melting point,
+    T - Tmelt = -cooling_rate * t, which nucleation reads."""
     os.makedirs(folder, exist_ok=True)
     nxm, nym, nzm, ntm = macro
     BC = Lx / (nxm - 3)
@@ -70,7 +76,10 @@ def write_line_forcing(folder, Lx, Ly, Lz, num_grains, seed, G, R, z0, top, t_en
     put("G.txt", [G])
     put("Rmax.txt", [R])
     put("V.txt", [0.0])
-    put("Nmax.txt", [0.01])
+    put("Nmax.txt", [nmax])
+    if cooling_rate is not None:
+        temp = np.broadcast_to(-cooling_rate * t[:, None, None, None], (ntm, nzm, nym, nxm))
+        put("Temp.txt", temp)
     put("UC.txt", [uc])
     put("NG.txt", [num_grains], "%d")
     put("NN.txt", [2 * num_grains], "%d")

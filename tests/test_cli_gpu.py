@@ -36,3 +36,51 @@ def test_phase_field_cli_line_run(tmp_path, built):
         assert key in d.files, key
     assert d["tip_y"].shape == (3,)
     assert d["total_area"].reshape(3, 10)[0].sum() > 0
+
+
+def _nucleation_run(tmp_path, tag, n_flag, pre_mt):
+    """A 3-D (non-line) nucleation run of the executable: a uniform melt cooling
+    at 5e6 K/s (Temp.txt), nucleation density 1/um^3."""
+    Lx = 2.48
+    work = tmp_path / tag
+    folder = work / "forcing" / "case0"
+    preprocess.write_line_forcing(str(folder), Lx, Lx, 2 * Lx, num_grains=9, seed=0, G=1.0,
+                                  R=0.05, z0=0.6, top=0.3, t_end=5e-7, nmax=1.0,
+                                  cooling_rate=5e6)
+    preprocess.write_input_file(str(work / "line.py"), Lx, nts=2, asp_ratio_zx=2.0, num_pf=8,
+                                pre_mt=pre_mt)
+    out = work / "out"
+    out.mkdir()
+    exe = os.path.join(ROOT, "cupf_b200", "phase_field")
+    r = subprocess.run([exe, "line.py", "-s", "0", "-b", "110", "-n", str(n_flag), "-d", "0",
+                        "-o", str(out)], cwd=work, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr + r.stdout
+    files = sorted(os.listdir(out))
+    assert len(files) == 1 and "Mixed_density1.000000_grains" in files[0], files
+    return np.load(out / files[0]), files[0]
+
+
+def test_phase_field_cli_liquid_start_nucleation(tmp_path, built):
+    """-n 1 with preMt = 60: the liquid-start phase nucleates grains in an
+    all-liquid domain (APTPhaseField.cu:779-816), their ids label the initial
+    solid, and the main loop nucleates from the temperature table.  The draw is
+    keyed on (seed, coarse cell, step), so a second run is identical."""
+    d, name = _nucleation_run(tmp_path, "a", 1, 60)
+    g2p, vol = d["grainToPF"], d["volume"]
+    assert len(g2p) == len(vol) and len(g2p) > 0
+    assert np.all(g2p > 9)            # every grain was nucleated (ids past num_theta)
+    assert np.all(vol > 0)
+    assert name.split("_grains")[1].startswith(str(len(np.unique(g2p))) + "_")
+    d2, name2 = _nucleation_run(tmp_path, "b", 1, 60)
+    assert name2 == name
+    for k in d.files:
+        assert np.array_equal(d[k], d2[k]), k
+
+
+def test_phase_field_cli_nucleation_from_temperature_table(tmp_path, built):
+    """-n 2 without a liquid start: the initial solid keeps id 0 (no substrate
+    ids outside the line configuration) and grains nucleate in the melt as the
+    temperature table cools it (APTPhaseField.cu:866-870)."""
+    d, _ = _nucleation_run(tmp_path, "c", 2, 0)
+    g2p = d["grainToPF"]
+    assert len(g2p) > 0 and np.all(g2p > 9)
