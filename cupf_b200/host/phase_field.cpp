@@ -341,6 +341,15 @@ bool PhaseField::initField() {
       alpha[id] = 0;
     }
   }
+  // A 3-D run that is neither a line run nor pure nucleation may start from a
+  // full grain-id field: alpha3D.h5:/alpha of the additive-manufacturing driver
+  // (AdditiveManufacturing/PhaseFieldCpu.cpp:430-447), read here from
+  // alpha3D.txt, `length` ids in the grid layout (halos included), replacing the
+  // zeros above.  Without the file the ids stay 0, as in 3DgrainMPI.
+  if (!ds->pureNucleation && !ds->useLineConfig) {
+    const int n = read_input(mac.folder + "/alpha3D.txt", alpha.data(), (int)length);
+    if (n >= 0 && n < length) return setErr("alpha3D.txt must hold fnx*fny*fnz grain ids");
+  }
   if (std::fabs(p.order - 100.0f) < 1e-3f) {
     if (read_input(mac.folder + "/statTemp.txt", mac.psi_mac.data(), (int)mac.psi_mac.size()) < 1)
       return setErr("order 100 needs statTemp.txt");

@@ -4,6 +4,7 @@ arrives at the same parameters and initial state as the in-memory case builder
 (which restates the same derivation), up to the 5 significant digits the
 forcing files store."""
 import numpy as np
+import pytest
 
 from cupf_b200 import cases, host_api, preprocess
 
@@ -35,3 +36,29 @@ def test_setup_from_forcing_folder(tmp_path, monkeypatch, built):
     assert solid.sum() > 1000
     assert np.array_equal(alpha[solid], c.alpha[solid])
     assert np.all(alpha[inner & (phi <= -0.995)] == 0)
+
+
+def test_setup_reads_alpha3d_field(tmp_path, monkeypatch, built):
+    """A 3-D run (not line, not pure nucleation) takes its initial grain ids from
+    alpha3D.txt when the forcing folder has one (the additive-manufacturing
+    driver's alpha3D.h5, AdditiveManufacturing/PhaseFieldCpu.cpp:430-447), else
+    all ids are 0; a short file is an error."""
+    Lx = 2.48
+    folder = tmp_path / "forcing" / "case0"
+    preprocess.write_line_forcing(str(folder), Lx, Lx, 2 * Lx, num_grains=9, seed=0, G=1.0,
+                                  R=0.05, z0=0.6, top=0.3, t_end=5e-7)
+    preprocess.write_input_file(str(tmp_path / "line.py"), Lx, nts=2, asp_ratio_zx=2.0, num_pf=8)
+    monkeypatch.chdir(tmp_path)
+    dims, _, _, alpha = host_api.setup("line.py", str(folder), bc=(1, 1, 0))
+    assert not alpha.any()
+    L = int(dims[0]) * int(dims[1]) * int(dims[2])
+    ids = np.random.default_rng(1).integers(0, 10, L).astype(np.int32)
+    np.savetxt(folder / "alpha3D.txt", ids, fmt="%d")
+    _, _, _, alpha = host_api.setup("line.py", str(folder), bc=(1, 1, 0))
+    assert np.array_equal(alpha, ids)
+    # the line configuration and pure nucleation do not read it
+    _, _, _, alpha = host_api.setup("line.py", str(folder), bc=(1, 1, 0), pure_nucleation=True)
+    assert not alpha.any()
+    np.savetxt(folder / "alpha3D.txt", ids[:-1], fmt="%d")
+    with pytest.raises(RuntimeError, match="alpha3D"):
+        host_api.setup("line.py", str(folder), bc=(1, 1, 0))
