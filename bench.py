@@ -570,22 +570,40 @@ def main():
         torch.cuda.synchronize(device)
 
     barrier()
+    solver.active_cells()  # restart the counter of computed cells
     with ClockSampler(device) as clk:
         ms = solver.time_steps(args.steps)
     barrier()
+    active = solver.active_cells() / args.steps  # cells of the computed items per launch
     ms = max_over_ranks(pg, ms, "cuda")
     value = replica_throughput(ws, cells, args.steps, ms)
 
-    # roofline of the step kernel (the only kernel in the timed region)
+    # The same number of steps with every work item computed (the reference's full
+    # sweep, no quiet items left alone), continuing from the state reached above.
+    solver.set_skip_quiet(False)
+    solver.step(2)
+    barrier()
+    ms_full = max_over_ranks(pg, solver.time_steps(args.steps), "cuda")
+    solver.set_skip_quiet(True)
+
+    # roofline of the step kernel (the only kernel in the timed region): the
+    # algorithmic bytes are the slot pairs of the cells it computes, each read
+    # once and written once; the cells of quiet items are neither read nor written
     bytes_per_cell = 2 * NUM_PF * (8 if args.precision == "fp32" else 4)
     launch_s = ms / 1e3 / args.steps
-    achieved = cells * bytes_per_cell / launch_s / 1e9
+    achieved = active * bytes_per_cell / launch_s / 1e9
     peak, peak_kind = measured_peak()
     traffic = profile_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
                 "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
-                "algorithmic_bytes_per_launch": cells * bytes_per_cell}
+                "algorithmic_bytes_per_launch": active * bytes_per_cell,
+                "computed_cells_per_launch": active, "interior_cells": cells}
+    full_sweep = {"value": replica_throughput(ws, cells, args.steps, ms_full), "unit": UNIT,
+                  "ms_per_step": ms_full / args.steps,
+                  "hbm_gbs": cells * bytes_per_cell / (ms_full / 1e3 / args.steps) / 1e9,
+                  "note": "every work item computed, steps %d-%d" % (
+                      args.warmup + args.steps + 3, args.warmup + 2 * args.steps + 2)}
 
     # end to end through the C ABI with host buffers: a whole C2 simulation
     e2e = None
@@ -635,6 +653,7 @@ def main():
                 "config": workload_config({"parallelism": "replicas x%d" % ws,
                                            "storage": args.precision}),
                 "hbm_gbs": achieved, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "full_sweep": full_sweep,
                 "clocks": clk.summary(), "gpu_launches": args.steps,
                 "baseline_metric": "3D APT Mcell-upd/s & HBM GB/s, mixed vs FP32; served sims/hr,"
                                    " p50/p99 at <=1e-3 err"}

@@ -51,6 +51,13 @@ struct StepArgs {
   void* out;         // pair buffer written this step
   int* err;          // device error word (0 = ok)
   int* work;         // [next item, CTAs done] of the persistent launch (self-resetting)
+  // Quiet-item flags (NULL = off): per work item, 1 when every interior cell of
+  // the item holds only empty slots in that buffer.  quiet_in describes `in`,
+  // quiet_out describes `out` as it stands before this step and is rewritten
+  // for every item the step computes.
+  const uint8_t* quiet_in;
+  uint8_t* quiet_out;
+  unsigned long long* active_cells;  // cells of the computed items, accumulated (may be NULL)
 };
 
 // Boundary map of one coordinate (APTsetBC3D, APTPhaseField.cu:111-112,134-135,157-158):

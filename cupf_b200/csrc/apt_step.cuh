@@ -247,6 +247,7 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
 
   land(0);
   land(1);
+  bool live = false;  // this thread wrote an occupied slot or left one unwritten
 
   const int gx = x0 + tx, gy = y0 + ty;
   const bool valid = gx <= a.fnx - 2 && gy <= a.fny - 2;
@@ -464,21 +465,62 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
           int id = L[0];
 #pragma unroll
           for (int q = 1; q < NP; ++q) id = (j == q) ? L[q] : id;
-          outp[j * ss] = update_slot(j, id);
+          const P v = update_slot(j, id);
+          live |= S::id(v) != -1;
+          outp[j * ss] = v;
         }
+      } else {
+        live = true;
       }
     } else {
 #pragma unroll
       for (int j = 0; j < NP; ++j) {
-        if (j >= n)
+        if (j >= n) {
           outp[j * ss] = S::empty();
-        else if (upd)  // else the reference leaves the slot unwritten
-          outp[j * ss] = update_slot(j, L[j]);
+        } else if (upd) {
+          const P v = update_slot(j, L[j]);
+          live |= S::id(v) != -1;
+          outp[j * ss] = v;
+        } else {
+          live = true;  // the reference leaves the slot unwritten
+        }
       }
     }
   }
 
+  // record whether the item's output is all empty slots
+  if (__syncthreads_or(live ? 1 : 0) == 0) {
+    if (tid == 0 && a.quiet_out) a.quiet_out[(zci * a.nty + tyi) * a.ntx + txi] = 1;
+  } else if (tid == 0 && a.quiet_out) {
+    a.quiet_out[(zci * a.nty + tyi) * a.ntx + txi] = 0;
+  }
+  if (tid == 0 && a.active_cells) {
+    const int wx = min(TX, a.fnx - 1 - x0), wy = min(TY, a.fny - 1 - y0);
+    atomicAdd(a.active_cells, (unsigned long long)(wx * wy * (k_end - k_begin)));
+  }
+
   qbase = q0 + nplanes;
+}
+
+// True when the step may leave work item (txi, tyi, zci) alone: its cells in
+// the output buffer already hold only empty slots, and so do its cells and the
+// face-neighbour cells its 7-point stencil reads in the input buffer (the
+// neighbouring items across each face, or the items the boundary map sends a
+// halo cell to).  Every cell of such an item would be written empty again.
+__device__ __forceinline__ bool item_quiet(const StepArgs& a, int txi, int tyi, int zci) {
+  const int per = a.ntx * a.nty;
+  const int it = zci * per + tyi * a.ntx + txi;
+  if (!a.quiet_out[it] || !a.quiet_in[it]) return false;
+  auto q = [&](int tx, int ty, int zc) { return a.quiet_in[zc * per + ty * a.ntx + tx] != 0; };
+  const int x0 = 1 + TX * txi, x1 = min(x0 + TX - 1, a.fnx - 2);
+  const int y0 = 1 + TY * tyi, y1 = min(y0 + TY - 1, a.fny - 2);
+  const int k0 = 1 + a.zc * zci, k1 = min(k0 + a.zc, a.fnz - 1);
+  const int xl = bc_map(x0 - 1, a.fnx, a.bcX), xr = bc_map(x1 + 1, a.fnx, a.bcX);
+  const int yl = bc_map(y0 - 1, a.fny, a.bcY), yr = bc_map(y1 + 1, a.fny, a.bcY);
+  const int zl = bc_map(k0 - 1, a.fnz, a.bcZ), zu = bc_map(k1, a.fnz, a.bcZ);
+  return q((xl - 1) / TX, tyi, zci) && q((xr - 1) / TX, tyi, zci) && q(txi, (yl - 1) / TY, zci) &&
+         q(txi, (yr - 1) / TY, zci) && q(txi, tyi, (zl - 1) / a.zc) &&
+         q(txi, tyi, (zu - 1) / a.zc);
 }
 
 // Hand the CTA its next work item from the launch's atomic counter (-1 when
@@ -528,6 +570,7 @@ __global__ void __launch_bounds__(NTHREADS, step_min_blocks<NP, S>())
     if (it < 0) break;
     const int zci = it / per_chunk;
     const int r = it - zci * per_chunk;
+    if (a.quiet_out && item_quiet(a, r % a.ntx, r / a.ntx, zci)) continue;
     step_item<NP, S>(&tmap, a, r % a.ntx, r / a.ntx, zci, sm, qbase);
   }
   sm.drain();

@@ -91,6 +91,12 @@ struct cupf_apt_handle {
   int* err = nullptr;
   int* work = nullptr;  // persistent-launch work counter [next, done]
   int grid_cap = 0;     // resident CTAs of the step kernel (occupancy x SMs)
+  // quiet-item flags of each buffer (StepArgs::quiet_in/out), sized for the
+  // finest item grid (z chunks of one plane); all 0 = nothing known
+  uint8_t* quiet[2] = {nullptr, nullptr};
+  size_t quiet_cap = 0;
+  bool skip_quiet = true;
+  unsigned long long* active_cells = nullptr;
   // read-back scratch (reference layout, num_pf * length), allocated on first use
   float* xfer_ph = nullptr;
   int* xfer_id = nullptr;
@@ -188,7 +194,8 @@ static void free_handle(cupf_apt_handle* h) {
                   h->Z_mac, h->t_mac, h->psi_mac, h->T_3D, h->phi_m, h->alpha_m, h->err, h->work,
                   h->xfer_ph, h->xfer_id, h->layer_sums, h->alpha_full, h->loss_area,
                   h->counts, h->first, h->qoi_part, h->nucl_status, h->nucl_count,
-                  h->nucl_sphere, h->jcand, h->jcount, h->jdistinct};
+                  h->nucl_sphere, h->jcand, h->jcount, h->jdistinct, h->quiet[0], h->quiet[1],
+                  h->active_cells};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -298,6 +305,14 @@ static void set_zc(cupf_apt_handle* h, int zc) {
   h->ntx = (h->p.fnx - 2 + TX - 1) / TX;
   h->nty = (h->p.fny - 2 + TY - 1) / TY;
   h->nzc = (nz + h->zc - 1) / h->zc;
+}
+
+// Forget what the quiet-item flags say about both buffers: after anything but
+// the step writes the slot buffers, or when the item grid changes.
+static cupf_status invalidate_quiet(cupf_apt_handle* h) {
+  for (int b = 0; b < 2; ++b)
+    if (h->quiet[b]) CK(cudaMemsetAsync(h->quiet[b], 0, h->quiet_cap, h->stream));
+  return CUPF_OK;
 }
 
 // Resident CTAs per SM the step kernel is compiled for (step_min_blocks).
@@ -441,6 +456,13 @@ extern "C" cupf_status cupf_apt_create(const cupf_apt_params* p, const cupf_apt_
   TRY(cuda(cudaMemsetAsync(h->err, 0, sizeof(int), h->stream), "memset"));
   TRY(cuda(cudaMalloc((void**)&h->work, 2 * sizeof(int)), "work"));
   TRY(cuda(cudaMemsetAsync(h->work, 0, 2 * sizeof(int), h->stream), "memset"));
+  h->quiet_cap = (size_t)((p->fnx - 2 + TX - 1) / TX) * ((p->fny - 2 + TY - 1) / TY) * (p->fnz - 2);
+  for (int b = 0; b < 2; ++b) {
+    TRY(cuda(cudaMalloc((void**)&h->quiet[b], h->quiet_cap), "quiet flags"));
+    TRY(cuda(cudaMemsetAsync(h->quiet[b], 0, h->quiet_cap, h->stream), "memset"));
+  }
+  TRY(cuda(cudaMalloc((void**)&h->active_cells, sizeof(unsigned long long)), "counter"));
+  TRY(cuda(cudaMemsetAsync(h->active_cells, 0, sizeof(unsigned long long), h->stream), "memset"));
   TRY(cuda(cudaMalloc((void**)&h->layer_sums, p->fnz * sizeof(double)), "layer sums"));
   for (int b = 0; b < 2; ++b) TRY(make_tmap(h, b));
   const char* zc_env = getenv("CUPF_ZC");
@@ -464,7 +486,26 @@ extern "C" void* cupf_apt_stream(cupf_apt_handle* h) { return h ? (void*)h->stre
 extern "C" cupf_status cupf_apt_set_tuning(cupf_apt_handle* h, int32_t z_chunk) {
   if (!h) return fail(CUPF_ERR_INVALID, "null handle");
   if (z_chunk < 1) return fail(CUPF_ERR_INVALID, "z_chunk must be >= 1");
+  CK(cudaSetDevice(h->device));
   set_zc(h, z_chunk);
+  return invalidate_quiet(h);
+}
+
+extern "C" cupf_status cupf_apt_set_skip_quiet(cupf_apt_handle* h, int32_t enable) {
+  if (!h) return fail(CUPF_ERR_INVALID, "null handle");
+  CK(cudaSetDevice(h->device));
+  h->skip_quiet = enable != 0;
+  return invalidate_quiet(h);
+}
+
+extern "C" cupf_status cupf_apt_active_cells(cupf_apt_handle* h, uint64_t* cells) {
+  if (!h || !cells) return fail(CUPF_ERR_INVALID, "null argument");
+  CK(cudaSetDevice(h->device));
+  unsigned long long v = 0;
+  CK(cudaMemcpyAsync(&v, h->active_cells, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemsetAsync(h->active_cells, 0, sizeof(v), h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  *cells = v;
   return CUPF_OK;
 }
 
@@ -482,6 +523,7 @@ extern "C" cupf_status cupf_apt_init_from_argmax(cupf_apt_handle* h, const float
   LAUNCH_S(h, init_kernel, grid_for(L), 256, B<S>(h->buf[0]), B<S>(h->buf[1]), h->phi_m,
            h->alpha_m, h->g);
   CK(cudaGetLastError());
+  if (cupf_status st = invalidate_quiet(h)) return st;
   h->cur = 0;
   h->steps_done = 0;
   h->initialised = true;
@@ -514,6 +556,7 @@ extern "C" cupf_status cupf_apt_set_slots(cupf_apt_handle* h, const float* ph, c
   LAUNCH_S(h, import_kernel, grid_for(n), 256, B<S>(h->buf[0]), h->xfer_ph, h->xfer_id, h->g);
   LAUNCH_S(h, import_kernel, grid_for(n), 256, B<S>(h->buf[1]), h->xfer_ph, h->xfer_id, h->g);
   CK(cudaGetLastError());
+  if ((st = invalidate_quiet(h))) return st;
   h->cur = 0;
   h->steps_done = steps_done;
   h->initialised = true;
@@ -560,6 +603,11 @@ extern "C" cupf_status cupf_apt_step(cupf_apt_handle* h, int32_t nsteps,
     a.sr_key = (uint32_t)(h->steps_done + 1);
     a.in = h->buf[h->cur];
     a.out = h->buf[h->cur ^ 1];
+    if (h->skip_quiet) {
+      a.quiet_in = h->quiet[h->cur];
+      a.quiet_out = h->quiet[h->cur ^ 1];
+    }
+    a.active_cells = h->active_cells;
     cupf_status st = launch_step(h, a, h->tmap[h->cur]);
     if (st) return st;
     h->cur ^= 1;
@@ -787,6 +835,7 @@ extern "C" cupf_status cupf_apt_nucleate(cupf_apt_handle* h, int32_t use_initial
   NuclArgs a = nucl_args(h, use_initial_undercooling);
   LAUNCH_S(h, nucleate_kernel, grid_for(nc), 256, B<S>(h->buf[h->cur]), a);
   CK(cudaGetLastError());
+  if (cupf_status st = invalidate_quiet(h)) return st;
   if (total) {
     CK(cudaMemcpyAsync(total, h->nucl_count, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
@@ -857,6 +906,7 @@ extern "C" cupf_status cupf_apt_move_domain(cupf_apt_handle* h, int32_t* tip_fro
     *tip_front -= 1;
     *moved += 1;
   }
+  if (*moved && (st = invalidate_quiet(h))) return st;
   if ((st = fill_halo(h, h->cur))) return st;
   CK(cudaStreamSynchronize(h->stream));
   return check_err_word(h);

@@ -154,6 +154,16 @@ class APTSolver:
     def set_tuning(self, z_chunk):
         abi.check(self.L.cupf_apt_set_tuning(self.h, int(z_chunk)))
 
+    def set_skip_quiet(self, enable):
+        """Leave work items whose cells stay all-empty alone (default on)."""
+        abi.check(self.L.cupf_apt_set_skip_quiet(self.h, int(bool(enable))))
+
+    def active_cells(self):
+        """Cells of the computed (not quiet) work items since the last call."""
+        v = C.c_uint64()
+        abi.check(self.L.cupf_apt_active_cells(self.h, C.byref(v)))
+        return v.value
+
     @property
     def stream(self):
         return self.L.cupf_apt_stream(self.h)
