@@ -35,6 +35,7 @@ NUM_PF = 8
 GRAINS = 600
 SEED = 0
 CONFIG_STEPS = 2000
+SERVE_STEPS = 1000  # steps of each served request (the served-stream configuration)
 METRIC = "3D APT Mcell-upd/s"
 UNIT = "Mcell-upd/s"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -246,9 +247,9 @@ def run_serve(args):
                     now = time.perf_counter() - t0
                     while k < len(reqs) and reqs[k][0] <= now:
                         c = reqs[k][1]
-                        ids.append(srv.submit(c, CONFIG_STEPS))
+                        ids.append(srv.submit(c, SERVE_STEPS))
                         p = c.params
-                        cells += (p.fnx - 2) * (p.fny - 2) * (p.fnz - 2) * CONFIG_STEPS
+                        cells += (p.fnx - 2) * (p.fny - 2) * (p.fnz - 2) * SERVE_STEPS
                         k += 1
                     running, pending, _ = srv.pump()
                     if running == 0 and pending == 0 and k < len(reqs):
@@ -256,12 +257,28 @@ def run_serve(args):
             res = [srv.result(r) for r in ids]
             ttr = np.array([r["times"][2] - r["times"][0] for r in res])
             span = max(r["times"][2] for r in res) - min(r["times"][0] for r in res)
+            for r in ids:
+                srv.release(r)
+            # capacity: the same requests all submitted at once (the stream above is
+            # paced by its arrivals: 4/s x 1000 steps x 3.1 M cells on average, about
+            # 12 G cell-updates/s of offered load)
+            with ClockSampler(0) as clk_sat:
+                t1 = time.perf_counter()
+                sat = [srv.submit(c, SERVE_STEPS) for _, c in reqs]
+                srv.run_until_done(sat)
+                sat_span = time.perf_counter() - t1
+            for r in sat:
+                srv.release(r)
             lines.append({"metric": "served sims/hr", "impl": "cupf-serve", "precision": prec,
                           "value": len(res) / span * 3600.0, "unit": "sims/hr",
                           "p50_s": float(np.percentile(ttr, 50)),
                           "p99_s": float(np.percentile(ttr, 99)),
                           "mcell_upd_per_s": cells / span / 1e6, "requests": len(res),
-                          "arrival_rate_per_s": 4.0, "steps_per_request": CONFIG_STEPS,
+                          "arrival_rate_per_s": 4.0, "steps_per_request": SERVE_STEPS,
+                          "saturated": {"sims_per_hr": len(sat) / sat_span * 3600.0,
+                                        "mcell_upd_per_s": cells / sat_span / 1e6,
+                                        "seconds": sat_span, "clocks": clk_sat.summary(),
+                                        "note": "all requests submitted at once"},
                           "grids": [list(g) for g in SERVE_GRIDS], "clocks": clk.summary(),
                           "data": "synthetic Poisson stream, seed 0"})
             print(json.dumps(lines[-1]), flush=True)

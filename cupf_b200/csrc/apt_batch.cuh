@@ -18,6 +18,7 @@ namespace cupf {
 struct BatchSim {
   StepArgs a;          // in / out / t are filled per step from the fields below
   void* buf[2];
+  uint8_t* quiet[2];   // quiet-item flags of each buffer (StepArgs::quiet_in/out)
   long long steps;     // explicit steps done
   long long target;    // steps requested
   int cur;             // buffer holding the current state
@@ -44,10 +45,13 @@ __global__ void __launch_bounds__(NTHREADS, step_min_blocks<NP, S>())
     const int cur = sd->cur;
     a.in = sd->buf[cur];
     a.out = sd->buf[cur ^ 1];
+    a.quiet_in = sd->quiet[cur];
+    a.quiet_out = sd->quiet[cur ^ 1];
     a.use_iuc = sd->use_iuc;
     // t of step n (1-based) = (float)n * dt * tau0, as the single-simulation path
     a.t = __fmul_rn(__fmul_rn((float)(sd->steps + 1), a.dt), a.tau0);
     a.sr_key = (uint32_t)(sd->steps + 1);
+    if (a.quiet_out && item_quiet(a, w.y, w.z, w.w)) continue;
     step_item<NP, S>(tmaps + 2 * w.x + cur, a, w.y, w.z, w.w, sm, qbase);
   }
   sm.drain();

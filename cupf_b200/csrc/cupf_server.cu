@@ -77,6 +77,7 @@ struct Request {
   float* dphi = nullptr;
   int* dalpha = nullptr;
   float* ddummy = nullptr;
+  uint8_t* dquiet[2] = {nullptr, nullptr};  // quiet-item flags of each buffer
   size_t bytes = 0;
   int zc = 64, ntx = 0, nty = 0, nzc = 0;
   // results
@@ -132,20 +133,22 @@ static int gridn(long long n) {
 
 static void free_request_device(Request* r) {
   void* ptrs[] = {r->buf[0], r->buf[1], r->dx, r->dy, r->dz, r->dsint, r->dcost, r->dorient, r->dphi,
-                  r->dalpha, r->ddummy};
+                  r->dalpha, r->ddummy, r->dquiet[0], r->dquiet[1]};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   r->buf[0] = r->buf[1] = nullptr;
   r->dx = r->dy = r->dz = r->dsint = r->dcost = r->dorient = r->dphi = nullptr;
   r->dalpha = nullptr;
   r->ddummy = nullptr;
+  r->dquiet[0] = r->dquiet[1] = nullptr;
 }
 
 static size_t request_bytes(const cupf_apt_params& p, int pair_bytes, int num_pf) {
   const int palign = pair_bytes == 8 ? 2 : 4;
   const size_t xp = (p.fnx + palign - 1) / palign * palign;
   const size_t L = (size_t)p.fnx * p.fny * p.fnz;
-  return 2 * xp * p.fny * p.fnz * num_pf * pair_bytes + L * 8 + 4096;
+  const size_t quiet = 2 * (size_t)((p.fnx - 2 + TX - 1) / TX) * ((p.fny - 2 + TY - 1) / TY) * (p.fnz - 2);
+  return 2 * xp * p.fny * p.fnz * num_pf * pair_bytes + L * 8 + quiet + 4096;
 }
 
 // Pick the z chunk of a grid shape by timing the single-simulation step on a
@@ -224,6 +227,11 @@ static cupf_status admit(cupf_server* s, Request* r, int slot) {
   CK(cudaMemcpyAsync(r->dalpha, r->alpha.data(), L * sizeof(int), cudaMemcpyHostToDevice, st));
   CK(cudaMalloc((void**)&r->ddummy, 64 * sizeof(float)));
   CK(cudaMemsetAsync(r->ddummy, 0, 64 * sizeof(float), st));
+  const size_t nq = (size_t)r->ntx * r->nty * r->nzc;
+  for (int b = 0; b < 2; ++b) {
+    CK(cudaMalloc((void**)&r->dquiet[b], nq));
+    CK(cudaMemsetAsync(r->dquiet[b], 0, nq, st));
+  }
   r->bytes = request_bytes(p, s->pair_bytes, np);
   // initial state in both buffers
   e = with_fmt(s->cfg.precision, [&](auto tag) -> cupf_status {
@@ -305,6 +313,8 @@ static cupf_status admit(cupf_server* s, Request* r, int slot) {
   a.err = s->d_err;
   bs.buf[0] = r->buf[0];
   bs.buf[1] = r->buf[1];
+  bs.quiet[0] = r->dquiet[0];
+  bs.quiet[1] = r->dquiet[1];
   bs.steps = 0;
   bs.target = r->nsteps;
   bs.cur = 0;
