@@ -185,6 +185,24 @@ __global__ void shift_kernel(const typename S::T* __restrict__ src, typename S::
   }
 }
 
+// Quiet-item flags after the domain moved down by m planes (new plane k holds old
+// plane k + m, planes past the top are empty): an item is quiet when every item
+// that held its new planes was.  src: flags before the move, dst: after.
+static __global__ void quiet_shift_kernel(const uint8_t* __restrict__ src, uint8_t* dst, int per_chunk,
+                                          int nzc, int zc, int fnz, int m) {
+  const long long n = (long long)per_chunk * nzc;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(i / per_chunk), t = (int)(i - (long long)c * per_chunk);
+    const int k0 = 1 + zc * c, k1 = min(k0 + zc, fnz - 1);  // planes [k0, k1)
+    const int lo = k0 + m, hi = min(k1 - 1 + m, fnz - 2);   // old planes they hold
+    uint8_t q = 1;
+    for (int cc = (lo - 1) / zc; lo <= hi && cc <= (hi - 1) / zc; ++cc)
+      q &= src[(long long)cc * per_chunk + t];
+    dst[i] = q;
+  }
+}
+
 template <class S>
 __global__ void copy_interior_kernel(const typename S::T* __restrict__ src, typename S::T* dst,
                                      Grid g) {

@@ -52,7 +52,7 @@ struct StepArgs {
   int* err;          // device error word (0 = ok)
   int* work;         // [next item, CTAs done] of the persistent launch (self-resetting)
   // Quiet-item flags (NULL = off): per work item, 1 when every interior cell of
-  // the item holds only empty slots in that buffer.  quiet_in describes `in`,
+  // the item holds only exact empty pairs (id -1, phi -1) in that buffer.  quiet_in describes `in`,
   // quiet_out describes `out` as it stands before this step and is rewritten
   // for every item the step computes.
   const uint8_t* quiet_in;

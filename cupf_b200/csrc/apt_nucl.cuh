@@ -31,6 +31,10 @@ struct NuclArgs {
   const float* sphere;  // (2*pts+1)^3 nucleus profile: tanh(dx*((1+pts)/2 - r)/sqrt2)
   int* status;          // per coarse cell: 1 = solid / already nucleated
   int* count;           // nucleation events (accumulated)
+  // quiet-item flags of the buffer written (NULL = none kept): the items a
+  // nucleus reaches are marked not quiet; tile tw x th cells, z chunk zc
+  uint8_t* quiet;
+  int tw, th, zc, ntx, nty;
 };
 
 // interp4Dtemperature (devicefunc.cu_inl:32-83): quadrilinear in (x, y, z, t),
@@ -133,6 +137,12 @@ __global__ void nucleate_kernel(typename S::T* buf, NuclArgs a) {
           // `ph > -0.9999f` (a float literal, APTPhaseField.cu:524) == v > kDrop
           buf[o] = S::make(v, v > kDrop ? id : S::id(old));
         }
+    if (a.quiet) {
+      for (int qz = (gk - a.pts - 1) / a.zc; qz <= (gk + a.pts - 1) / a.zc; ++qz)
+        for (int qy = (gj - a.pts - 1) / a.th; qy <= (gj + a.pts - 1) / a.th; ++qy)
+          for (int qx = (gi - a.pts - 1) / a.tw; qx <= (gi + a.pts - 1) / a.tw; ++qx)
+            a.quiet[((long long)qz * a.nty + qy) * a.ntx + qx] = 0;
+    }
     a.status[C] = 1;
     atomicAdd(a.count, 1);
   }

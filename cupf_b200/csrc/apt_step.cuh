@@ -247,7 +247,9 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
 
   land(0);
   land(1);
-  bool live = false;  // this thread wrote an occupied slot or left one unwritten
+  // this thread wrote a slot other than the exact empty pair (an occupied slot, or
+  // one whose id was just dropped: it keeps its last phi) or left one unwritten
+  bool live = false;
 
   const int gx = x0 + tx, gy = y0 + ty;
   const bool valid = gx <= a.fnx - 2 && gy <= a.fny - 2;
@@ -466,7 +468,7 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
 #pragma unroll
           for (int q = 1; q < NP; ++q) id = (j == q) ? L[q] : id;
           const P v = update_slot(j, id);
-          live |= S::id(v) != -1;
+          live |= !S::is_empty(v);
           outp[j * ss] = v;
         }
       } else {
@@ -479,7 +481,7 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
           outp[j * ss] = S::empty();
         } else if (upd) {
           const P v = update_slot(j, L[j]);
-          live |= S::id(v) != -1;
+          live |= !S::is_empty(v);
           outp[j * ss] = v;
         } else {
           live = true;  // the reference leaves the slot unwritten
@@ -503,10 +505,11 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
 }
 
 // True when the step may leave work item (txi, tyi, zci) alone: its cells in
-// the output buffer already hold only empty slots, and so do its cells and the
-// face-neighbour cells its 7-point stencil reads in the input buffer (the
-// neighbouring items across each face, or the items the boundary map sends a
-// halo cell to).  Every cell of such an item would be written empty again.
+// the output buffer already hold only exact empty pairs (id -1, phi -1), and its
+// cells and the face-neighbour cells its 7-point stencil reads in the input
+// buffer hold no id (the neighbouring items across each face, or the items the
+// boundary map sends a halo cell to).  Every cell of such an item would be
+// written as the empty pair again.
 __device__ __forceinline__ bool item_quiet(const StepArgs& a, int txi, int tyi, int zci) {
   const int per = a.ntx * a.nty;
   const int it = zci * per + tyi * a.ntx + txi;

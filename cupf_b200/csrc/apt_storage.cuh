@@ -33,6 +33,7 @@ struct PairF32 {
   __host__ __device__ static int id(T p) { return (int)p.y; }
   __device__ static T make(float ph, int id) { return make_uint2(__float_as_uint(ph), (uint32_t)id); }
   __device__ static T empty() { return make_uint2(0xBF800000u, 0xFFFFFFFFu); }
+  __device__ static bool is_empty(T p) { return p.x == 0xBF800000u && p.y == 0xFFFFFFFFu; }
   static constexpr bool kStochastic = false;
   __device__ static T make_sr(float ph, int id, uint32_t) { return make(ph, id); }
 };
@@ -86,6 +87,7 @@ struct PairH16 {
     return (uint32_t)encode(ph) | ((uint32_t)(unsigned short)(short)id << 16);
   }
   __device__ static T empty() { return 0xFFFF8000u; }  // u = -0 (phi = -1), id -1
+  __device__ static bool is_empty(T p) { return p == 0xFFFF8000u; }
 };
 
 using PairBF16 = PairH16<Half16::BF16>;

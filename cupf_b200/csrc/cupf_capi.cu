@@ -776,6 +776,12 @@ static NuclArgs nucl_args(cupf_apt_handle* h, int use_iuc) {
   a.sphere = h->nucl_sphere;
   a.status = h->nucl_status;
   a.count = h->nucl_count;
+  a.quiet = h->quiet[h->cur];
+  a.tw = TX;
+  a.th = TY;
+  a.zc = h->zc;
+  a.ntx = h->ntx;
+  a.nty = h->nty;
   return a;
 }
 
@@ -835,7 +841,6 @@ extern "C" cupf_status cupf_apt_nucleate(cupf_apt_handle* h, int32_t use_initial
   NuclArgs a = nucl_args(h, use_initial_undercooling);
   LAUNCH_S(h, nucleate_kernel, grid_for(nc), 256, B<S>(h->buf[h->cur]), a);
   CK(cudaGetLastError());
-  if (cupf_status st = invalidate_quiet(h)) return st;
   if (total) {
     CK(cudaMemcpyAsync(total, h->nucl_count, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
@@ -906,7 +911,16 @@ extern "C" cupf_status cupf_apt_move_domain(cupf_apt_handle* h, int32_t* tip_fro
     *tip_front -= 1;
     *moved += 1;
   }
-  if (*moved && (st = invalidate_quiet(h))) return st;
+  if (*moved) {
+    // both buffers now hold the shifted state: shift the current buffer's flags
+    // into the other one and copy them back
+    const int per = h->ntx * h->nty;
+    quiet_shift_kernel<<<grid_for((long long)per * h->nzc), 256, 0, h->stream>>>(
+        h->quiet[h->cur], h->quiet[h->cur ^ 1], per, h->nzc, h->zc, p.fnz, *moved);
+    CK(cudaMemcpyAsync(h->quiet[h->cur], h->quiet[h->cur ^ 1], (size_t)per * h->nzc,
+                       cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaGetLastError());
+  }
   if ((st = fill_halo(h, h->cur))) return st;
   CK(cudaStreamSynchronize(h->stream));
   return check_err_word(h);

@@ -284,14 +284,15 @@ void* cupf_apt_stream(cupf_apt_handle* h);
 cupf_status cupf_apt_set_tuning(cupf_apt_handle* h, int32_t z_chunk);
 
 /* Quiet work items (on by default).  The step keeps, per work item and buffer, a
- * flag that the item's cells hold only empty slots, and leaves an item alone
- * when its cells in the buffer it writes are already empty and its cells and
- * their face neighbours in the buffer it reads are too: every cell of such an
+ * flag that every slot of the item's cells holds the empty pair (id -1, phi -1),
+ * and leaves an item alone when its cells in the buffer it writes are already
+ * empty and its cells and their face neighbours in the buffer it reads are too:
+ * every cell of such an
  * item would be written empty again (APTrhs_psi on a cell whose 7 stencil
  * points hold no id, APTPhaseField.cu:198-233), so results are identical with
  * and without it.  enable = 0 computes every item (the reference's full sweep).
- * Anything else that writes the slot buffers (init, set_slots, nucleation, a
- * domain shift) and set_tuning reset the flags. */
+ * Init, set_slots and set_tuning reset the flags; a nucleation pass marks the
+ * items its nuclei reach, and a domain shift moves the flags with the planes. */
 cupf_status cupf_apt_set_skip_quiet(cupf_apt_handle* h, int32_t enable);
 
 /* Cells of the work items the step computed (not left alone as quiet) since the

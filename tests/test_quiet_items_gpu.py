@@ -66,3 +66,44 @@ def test_skip_follows_the_front(built):
     assert np.array_equal(a_id, b_id)
     assert np.array_equal(a_ph.view(np.int32), b_ph.view(np.int32))
     assert a_cells < 32 * 16 * 48 * 400
+
+
+def test_skip_across_nucleation_and_domain_shifts(built):
+    """Nucleation marks the items a nucleus reaches, and a domain shift moves the
+    flags down with the planes; both paths keep the skip exact: a liquid-start
+    run with nuclei landing in quiet melt, then moving-domain steps, agrees bit
+    for bit with the full sweep."""
+    c = cases.line_case(40, 24, 64, num_pf=5, num_grains=8, seed=7, bc="110", z0_frac=0.8)
+    p = c.params
+    p.nuc_rad = np.float32(0.16)
+    p.pts_cell = int(np.float32(0.16) / np.float32(np.float32(0.8) * np.float32(0.1)))
+    p.nuc_Nmax0 = np.float32(5.0)
+    p.nuc_Nmax = np.float32(5.0)
+    p.seed = 5
+    ph0, id0 = c.initial_slots()
+    out = []
+    for skip in (True, False):
+        with APTSolver(c) as s:
+            s.set_slots(ph0, id0, 0)
+            s.set_tuning(2)
+            s.set_skip_quiet(skip)
+            s.nucl_init()
+            total = 0
+            for _ in range(30):
+                s.step(1, True)
+                total = s.nucleate(True)
+                s.step(1, True)
+            tip, mc, moved_total = 1, 0, 0
+            for _ in range(20):
+                s.step(10)
+                tip, mc, moved = s.move_domain(tip, int(0.8 * p.fnz), mc)
+                moved_total += moved
+            s.step(20)
+            ph, ids = s.get_slots()
+            out.append((ph, ids, total, moved_total, s.active_cells()))
+    (a_ph, a_id, a_n, a_m, a_cells), (b_ph, b_id, b_n, b_m, b_cells) = out
+    assert a_n == b_n and a_n > 0
+    assert a_m == b_m and a_m > 0
+    assert np.array_equal(a_id, b_id)
+    assert np.array_equal(a_ph.view(np.int32), b_ph.view(np.int32))
+    assert a_cells < b_cells
