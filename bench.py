@@ -262,11 +262,13 @@ def run_serve(args):
             # capacity: the same requests all submitted at once (the stream above is
             # paced by its arrivals: 4/s x 1000 steps x 3.1 M cells on average, about
             # 12 G cell-updates/s of offered load)
+            busy0, _ = srv.stats()
             with ClockSampler(0) as clk_sat:
                 t1 = time.perf_counter()
                 sat = [srv.submit(c, SERVE_STEPS) for _, c in reqs]
                 srv.run_until_done(sat)
                 sat_span = time.perf_counter() - t1
+            busy = (srv.stats()[0] - busy0) / 1e3
             for r in sat:
                 srv.release(r)
             lines.append({"metric": "served sims/hr", "impl": "cupf-serve", "precision": prec,
@@ -277,7 +279,8 @@ def run_serve(args):
                           "arrival_rate_per_s": 4.0, "steps_per_request": SERVE_STEPS,
                           "saturated": {"sims_per_hr": len(sat) / sat_span * 3600.0,
                                         "mcell_upd_per_s": cells / sat_span / 1e6,
-                                        "seconds": sat_span, "clocks": clk_sat.summary(),
+                                        "seconds": sat_span, "device_busy_s": busy,
+                                        "clocks": clk_sat.summary(),
                                         "note": "all requests submitted at once"},
                           "grids": [list(g) for g in SERVE_GRIDS], "clocks": clk.summary(),
                           "data": "synthetic Poisson stream, seed 0"})

@@ -154,6 +154,7 @@ def lib():
                                    C.POINTER(C.c_int64), C.c_int32, C.POINTER(C.c_double),
                                    C.POINTER(C.c_double)],
             "cupf_server_release": [vp, C.c_int64],
+            "cupf_server_stats": [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64)],
             "cupf_ek2d_derive": [C.POINTER(cupf_ek2d_params), C.c_float],
             "cupf_ek2d_parse_input": [C.c_char_p, C.POINTER(cupf_ek2d_params),
                                       C.POINTER(C.c_int32), C.POINTER(C.c_int32), FP],

@@ -77,6 +77,13 @@ class Server:
             return None
         return {"alpha": alpha, "volumes": vols, "qoi": tuple(qoi), "times": tuple(times)}
 
+    def stats(self):
+        """(device ms of the rounds waited for so far, rounds launched)."""
+        ms = C.c_double()
+        n = C.c_int64()
+        abi.check(self.L.cupf_server_stats(self.h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
     def release(self, rid):
         abi.check(self.L.cupf_server_release(self.h, rid))
         self.meta.pop(rid, None)

@@ -330,8 +330,16 @@ cupf_status cupf_server_submit(cupf_server* s, const cupf_apt_params* p,
                                const cupf_apt_inputs* in, const float* phi,
                                const int32_t* alpha, int64_t nsteps, int64_t* request_id);
 
-/* One scheduling round (see above); blocks until the round's steps are done.
- * Any output pointer may be NULL. */
+/* Device time of the rounds waited for so far (CUDA events around each round's
+ * graph launch, ms) and the number of rounds launched.  Either pointer may be
+ * NULL. */
+cupf_status cupf_server_stats(cupf_server* s, double* busy_ms, int64_t* rounds);
+
+/* One scheduling round (see above).  It first waits for the previous round's
+ * steps, retires and admits, then launches this round's steps and returns
+ * without waiting for them, so the caller's own work between rounds overlaps
+ * the device.  Counts are those after admission.  Any output pointer may be
+ * NULL. */
 cupf_status cupf_server_pump(cupf_server* s, int32_t* n_running, int32_t* n_pending,
                              int32_t* n_done);
 
