@@ -187,7 +187,8 @@ __global__ void shift_kernel(const typename S::T* __restrict__ src, typename S::
 
 // Quiet-item flags after the domain moved down by m planes (new plane k holds old
 // plane k + m, planes past the top are empty): an item is quiet when every item
-// that held its new planes was.  src: flags before the move, dst: after.
+// that held its new planes was (bit 0; bits 1 and 2, its bottom and top plane,
+// are set only with bit 0).  src: flags before the move, dst: after.
 static __global__ void quiet_shift_kernel(const uint8_t* __restrict__ src, uint8_t* dst, int per_chunk,
                                           int nzc, int zc, int fnz, int m) {
   const long long n = (long long)per_chunk * nzc;
@@ -198,8 +199,8 @@ static __global__ void quiet_shift_kernel(const uint8_t* __restrict__ src, uint8
     const int lo = k0 + m, hi = min(k1 - 1 + m, fnz - 2);   // old planes they hold
     uint8_t q = 1;
     for (int cc = (lo - 1) / zc; lo <= hi && cc <= (hi - 1) / zc; ++cc)
-      q &= src[(long long)cc * per_chunk + t];
-    dst[i] = q;
+      q &= src[(long long)cc * per_chunk + t] & 1;
+    dst[i] = q ? 7 : 0;  // plane bits only from a wholly empty item
   }
 }
 

@@ -51,8 +51,9 @@ struct StepArgs {
   void* out;         // pair buffer written this step
   int* err;          // device error word (0 = ok)
   int* work;         // [next item, CTAs done] of the persistent launch (self-resetting)
-  // Quiet-item flags (NULL = off): per work item, 1 when every interior cell of
-  // the item holds only exact empty pairs (id -1, phi -1) in that buffer.  quiet_in describes `in`,
+  // Quiet-item flags (NULL = off): per work item, bit 0 set when every interior
+  // cell of the item holds only exact empty pairs (id -1, phi -1) in that
+  // buffer, bits 1 and 2 the same for its bottom and its top plane.  quiet_in describes `in`,
   // quiet_out describes `out` as it stands before this step and is rewritten
   // for every item the step computes.
   const uint8_t* quiet_in;

@@ -247,9 +247,10 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
 
   land(0);
   land(1);
-  // this thread wrote a slot other than the exact empty pair (an occupied slot, or
-  // one whose id was just dropped: it keeps its last phi) or left one unwritten
-  bool live = false;
+  // bit 0: this thread wrote a slot other than the exact empty pair (an occupied
+  // slot, or one whose id was just dropped: it keeps its last phi) or left one
+  // unwritten; bits 1 and 2: the same in the item's bottom and top plane
+  uint32_t live = 0;
 
   const int gx = x0 + tx, gy = y0 + ty;
   const bool valid = gx <= a.fnx - 2 && gy <= a.fny - 2;
@@ -292,6 +293,7 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
     mk[6] = masks[sU * BCELLS + c];
 
     P* outp = gout + (long long)k * plane_pairs + (long long)gy * a.xp + gx;
+    bool clive = false;
     const uint32_t any = mk[0] | mk[1] | mk[2] | mk[3] | mk[4] | mk[5] | mk[6];
     if (any == 0) {
       const P empty = S::empty();
@@ -468,11 +470,11 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
 #pragma unroll
           for (int q = 1; q < NP; ++q) id = (j == q) ? L[q] : id;
           const P v = update_slot(j, id);
-          live |= !S::is_empty(v);
+          clive |= !S::is_empty(v);
           outp[j * ss] = v;
         }
       } else {
-        live = true;
+        clive = true;
       }
     } else {
 #pragma unroll
@@ -481,21 +483,23 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
           outp[j * ss] = S::empty();
         } else if (upd) {
           const P v = update_slot(j, L[j]);
-          live |= !S::is_empty(v);
+          clive |= !S::is_empty(v);
           outp[j * ss] = v;
         } else {
-          live = true;  // the reference leaves the slot unwritten
+          clive = true;  // the reference leaves the slot unwritten
         }
       }
     }
+    if (clive) live |= 1u | (k == k_begin ? 2u : 0u) | (k == k_end - 1 ? 4u : 0u);
   }
 
-  // record whether the item's output is all empty slots
-  if (__syncthreads_or(live ? 1 : 0) == 0) {
-    if (tid == 0 && a.quiet_out) a.quiet_out[(zci * a.nty + tyi) * a.ntx + txi] = 1;
-  } else if (tid == 0 && a.quiet_out) {
-    a.quiet_out[(zci * a.nty + tyi) * a.ntx + txi] = 0;
-  }
+  // record which of the item's output, its bottom plane and its top plane hold
+  // only exact empty pairs (flag bits 0, 1, 2)
+  const int busy = __syncthreads_or(live & 1u), busy_lo = __syncthreads_or(live & 2u),
+            busy_hi = __syncthreads_or(live & 4u);
+  if (tid == 0 && a.quiet_out)
+    a.quiet_out[(zci * a.nty + tyi) * a.ntx + txi] =
+        (uint8_t)((busy ? 0 : 1) | (busy_lo ? 0 : 2) | (busy_hi ? 0 : 4));
   if (tid == 0 && a.active_cells) {
     const int wx = min(TX, a.fnx - 1 - x0), wy = min(TY, a.fny - 1 - y0);
     atomicAdd(a.active_cells, (unsigned long long)(wx * wy * (k_end - k_begin)));
@@ -507,23 +511,31 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
 // True when the step may leave work item (txi, tyi, zci) alone: its cells in
 // the output buffer already hold only exact empty pairs (id -1, phi -1), and its
 // cells and the face-neighbour cells its 7-point stencil reads in the input
-// buffer hold no id (the neighbouring items across each face, or the items the
-// boundary map sends a halo cell to).  Every cell of such an item would be
-// written as the empty pair again.
+// buffer hold no id.  Those neighbours are the whole items across the x and y
+// faces (or the items the boundary map sends a halo cell to), and across the z
+// faces the top plane of the item below and the bottom plane of the item above
+// (flag bits 2 and 1; a halo plane maps to an arbitrary plane, so there the
+// whole item's bit 0).  Every cell of such an item would be written as the empty
+// pair again.
 __device__ __forceinline__ bool item_quiet(const StepArgs& a, int txi, int tyi, int zci) {
   const int per = a.ntx * a.nty;
   const int it = zci * per + tyi * a.ntx + txi;
-  if (!a.quiet_out[it] || !a.quiet_in[it]) return false;
-  auto q = [&](int tx, int ty, int zc) { return a.quiet_in[zc * per + ty * a.ntx + tx] != 0; };
+  if (!(a.quiet_out[it] & 1) || !(a.quiet_in[it] & 1)) return false;
+  auto q = [&](int tx, int ty, int zc, int bit) {
+    return (a.quiet_in[zc * per + ty * a.ntx + tx] & bit) != 0;
+  };
   const int x0 = 1 + TX * txi, x1 = min(x0 + TX - 1, a.fnx - 2);
   const int y0 = 1 + TY * tyi, y1 = min(y0 + TY - 1, a.fny - 2);
   const int k0 = 1 + a.zc * zci, k1 = min(k0 + a.zc, a.fnz - 1);
   const int xl = bc_map(x0 - 1, a.fnx, a.bcX), xr = bc_map(x1 + 1, a.fnx, a.bcX);
   const int yl = bc_map(y0 - 1, a.fny, a.bcY), yr = bc_map(y1 + 1, a.fny, a.bcY);
-  const int zl = bc_map(k0 - 1, a.fnz, a.bcZ), zu = bc_map(k1, a.fnz, a.bcZ);
-  return q((xl - 1) / TX, tyi, zci) && q((xr - 1) / TX, tyi, zci) && q(txi, (yl - 1) / TY, zci) &&
-         q(txi, (yr - 1) / TY, zci) && q(txi, tyi, (zl - 1) / a.zc) &&
-         q(txi, tyi, (zu - 1) / a.zc);
+  const bool below = k0 - 1 >= 1
+                         ? q(txi, tyi, zci - 1, 4)
+                         : q(txi, tyi, (bc_map(k0 - 1, a.fnz, a.bcZ) - 1) / a.zc, 1);
+  const bool above = k1 <= a.fnz - 2 ? q(txi, tyi, zci + 1, 2)
+                                     : q(txi, tyi, (bc_map(k1, a.fnz, a.bcZ) - 1) / a.zc, 1);
+  return below && above && q((xl - 1) / TX, tyi, zci, 1) && q((xr - 1) / TX, tyi, zci, 1) &&
+         q(txi, (yl - 1) / TY, zci, 1) && q(txi, (yr - 1) / TY, zci, 1);
 }
 
 // Hand the CTA its next work item from the launch's atomic counter (-1 when
