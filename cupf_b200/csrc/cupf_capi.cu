@@ -96,6 +96,7 @@ struct cupf_apt_handle {
   uint8_t* quiet[2] = {nullptr, nullptr};
   size_t quiet_cap = 0;
   bool skip_quiet = true;
+  bool zc_user = false;  // z chunk fixed by the caller (set_tuning or CUPF_ZC)
   unsigned long long* active_cells = nullptr;
   // read-back scratch (reference layout, num_pf * length), allocated on first use
   float* xfer_ph = nullptr;
@@ -351,6 +352,37 @@ static int default_zc(cupf_apt_handle* h) {
   return 1;
 }
 
+// z chunk for a state whose grain ids occupy nz_active interior planes (those
+// within 10 planes of a plane holding an id: the tails the first steps grow):
+// the largest of 16, 8, 4, 2 that gives at least 2 work items per resident CTA
+// over those planes, else 1.  Quiet items cost next to nothing, so the items
+// that count are the ones the step computes.  Measured on line cases (B200,
+// NUM_PF = 8, FP32 and FP16, 64^3 to 256x256x512): within 6 % of the best chunk
+// of 16..1 on every case, where sizing by all items was up to 18 % off.
+static int zc_for_active(cupf_apt_handle* h, int nz_active) {
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+  const long long tiles = (long long)((h->p.fnx - 2 + TX - 1) / TX) * ((h->p.fny - 2 + TY - 1) / TY);
+  const long long want = 2LL * resident_per_sm(h) * nsm;
+  for (int zc = 16; zc > 1; zc /= 2)
+    if (tiles * ((nz_active + zc - 1) / zc) >= want) return zc;
+  return 1;
+}
+
+// Interior planes within 10 planes of a plane that holds an id (plane_any[k]
+// for k = 0..fnz-1); all interior planes when none does.
+static int active_planes(const std::vector<char>& plane_any, int fnz) {
+  const int nz = fnz - 2, reach = 10;
+  int n = 0, last = -1000000;
+  std::vector<int> next(fnz + 1, 1000000);
+  for (int k = fnz - 1; k >= 0; --k) next[k] = plane_any[k] ? k : next[k + 1];
+  for (int k = 1; k <= nz; ++k) {
+    if (plane_any[k]) last = k;
+    if (k - last <= reach || next[k] - k <= reach) ++n;
+  }
+  return n > 0 ? n : nz;
+}
+
 static int grid_for(long long n, int block = 256) {
   long long b = (n + block - 1) / block;
   if (b > 148 * 16) b = 148 * 16;
@@ -466,6 +498,7 @@ extern "C" cupf_status cupf_apt_create(const cupf_apt_params* p, const cupf_apt_
   TRY(cuda(cudaMalloc((void**)&h->layer_sums, p->fnz * sizeof(double)), "layer sums"));
   for (int b = 0; b < 2; ++b) TRY(make_tmap(h, b));
   const char* zc_env = getenv("CUPF_ZC");
+  h->zc_user = zc_env != nullptr;
   set_zc(h, zc_env ? atoi(zc_env) : default_zc(h));
   TRY(cuda(cudaStreamSynchronize(h->stream), "sync"));
 #undef TRY
@@ -488,6 +521,7 @@ extern "C" cupf_status cupf_apt_set_tuning(cupf_apt_handle* h, int32_t z_chunk) 
   if (z_chunk < 1) return fail(CUPF_ERR_INVALID, "z_chunk must be >= 1");
   CK(cudaSetDevice(h->device));
   set_zc(h, z_chunk);
+  h->zc_user = true;
   return invalidate_quiet(h);
 }
 
@@ -518,6 +552,17 @@ extern "C" cupf_status cupf_apt_init_from_argmax(cupf_apt_handle* h, const float
   for (size_t i = 0; i < L; ++i)
     if ((double)phi[i] > LS && (alpha[i] < -1 || alpha[i] > id_max))
       return fail(CUPF_ERR_INVALID, "grain id %d at %zu outside [-1, %d]", alpha[i], i, id_max);
+  if (!h->zc_user) {
+    std::vector<char> plane_any(h->p.fnz, 0);
+    for (int k = 1; k < h->p.fnz - 1; ++k)
+      for (int j = 1; j < h->p.fny - 1 && !plane_any[k]; ++j)
+        for (int i = 1; i < h->p.fnx - 1; ++i)
+          if ((double)phi[(size_t)k * h->p.fnx * h->p.fny + (size_t)j * h->p.fnx + i] > LS) {
+            plane_any[k] = 1;
+            break;
+          }
+    set_zc(h, zc_for_active(h, active_planes(plane_any, h->p.fnz)));
+  }
   CK(cudaMemcpyAsync(h->phi_m, phi, L * sizeof(float), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->alpha_m, alpha, L * sizeof(int), cudaMemcpyHostToDevice, h->stream));
   LAUNCH_S(h, init_kernel, grid_for(L), 256, B<S>(h->buf[0]), B<S>(h->buf[1]), h->phi_m,
@@ -544,11 +589,26 @@ extern "C" cupf_status cupf_apt_set_slots(cupf_apt_handle* h, const float* ph, c
                                           int64_t steps_done) {
   if (!h || !ph || !ids) return fail(CUPF_ERR_INVALID, "null argument");
   CK(cudaSetDevice(h->device));
-  const size_t n = (size_t)h->g.length() * h->g.np;
+  const size_t L = (size_t)h->g.length();
+  const size_t n = L * h->g.np;
   const int id_max = h->prec == CUPF_PREC_FP32 ? 0x7FFFFFFF : 32767;
   for (size_t i = 0; i < n; ++i)
     if (ids[i] < -1 || ids[i] > id_max)
       return fail(CUPF_ERR_INVALID, "grain id %d at %zu outside [-1, %d]", ids[i], i, id_max);
+  if (!h->zc_user) {
+    // reference layout: index = i + j*fnx + k*fnx*fny + slot*L
+    std::vector<char> plane_any(h->p.fnz, 0);
+    const int fnx = h->p.fnx, fny = h->p.fny;
+    for (int p = 0; p < h->g.np; ++p)
+      for (int k = 1; k < h->p.fnz - 1; ++k)
+        for (int j = 1; j < fny - 1 && !plane_any[k]; ++j)
+          for (int i = 1; i < fnx - 1; ++i)
+            if (ids[p * L + (size_t)k * fnx * fny + (size_t)j * fnx + i] >= 0) {
+              plane_any[k] = 1;
+              break;
+            }
+    set_zc(h, zc_for_active(h, active_planes(plane_any, h->p.fnz)));
+  }
   cupf_status st = ensure_xfer(h);
   if (st) return st;
   CK(cudaMemcpyAsync(h->xfer_ph, ph, n * sizeof(float), cudaMemcpyHostToDevice, h->stream));

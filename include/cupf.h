@@ -280,7 +280,10 @@ void* cupf_apt_stream(cupf_apt_handle* h);
 
 /* Launch shape of the step kernel: z_chunk = interior planes per CTA work item
  * (the column tile is fixed at 32 x 8).  No reference counterpart (the
- * reference marches every column over the whole height, APTPhaseField.cu:190). */
+ * reference marches every column over the whole height, APTPhaseField.cu:190).
+ * Without this call (or the CUPF_ZC environment variable) the library picks the
+ * chunk whenever a state is loaded (init_from_argmax, set_slots) from the
+ * planes that hold grain ids; after it, the given chunk stays. */
 cupf_status cupf_apt_set_tuning(cupf_apt_handle* h, int32_t z_chunk);
 
 /* Quiet work items (on by default).  The step keeps, per work item and buffer, a
