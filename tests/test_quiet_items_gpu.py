@@ -107,3 +107,25 @@ def test_skip_across_nucleation_and_domain_shifts(built):
     assert np.array_equal(a_id, b_id)
     assert np.array_equal(a_ph.view(np.int32), b_ph.view(np.int32))
     assert a_cells < b_cells
+
+
+def test_skip_matches_full_sweep_on_the_benchmark_workload(built):
+    """The benchmark's own case (256x256x512, 600 grains, NUM_PF = 8, FP32) over a
+    whole 2000-step run: argmax map, phi and the FP64 interface sums are the same
+    with quiet items left alone and with every item computed."""
+    c = cases.line_case(256, 256, 512, num_pf=8, num_grains=600, seed=0, bc="110")
+    out = []
+    for skip in (True, False):
+        with APTSolver(c) as s:
+            s.init_from_argmax(c.phi, c.alpha)
+            s.set_skip_quiet(skip)
+            s.active_cells()
+            s.step(2000)
+            cells = s.active_cells()
+            phi, alpha = s.collect(clear=True)
+            out.append((phi, alpha, s.qoi_sums(), cells))
+    (pa, aa, qa, ca), (pb, ab, qb, cb) = out
+    assert np.array_equal(aa, ab)
+    assert np.array_equal(pa.view(np.int32), pb.view(np.int32))
+    assert tuple(qa) == tuple(qb)
+    assert ca < 0.4 * cb
