@@ -7,11 +7,22 @@ NUM_PF = 8 slots, FP32 storage, periodic x/y and no-flux z; synthetic seeded
 inputs of the reference's shapes (the reference ships no dataset).
 
 A "step" is one explicit time step of the whole grid (one launch of the fused
-step kernel).  `value` = interior cells x K / device time of K steps (CUDA events
-on the solver's stream, inputs resident in HBM; the 4.4 GB of pair buffers are
-far larger than L2, so no flush is needed).  `e2e` = the same metric through the
-C ABI with host buffers: initial fields host->device, all steps of the
-configuration (2000), argmax map and grain volumes device->host.
+step kernel) with every work item computed, as the reference sweeps every cell.
+`value` = interior cells x K / device time of K steps (CUDA events on the
+solver's stream, inputs resident in HBM; the 4.4 GB of pair buffers are far
+larger than L2, so no flush is needed).  `quiet_skip` times the same K steps from
+the same state with the library's default of leaving alone work items whose
+cells stay exact empty pairs (bit-identical results).  `e2e` = the same metric
+through the C ABI with host buffers: initial fields host->device, all steps of
+the configuration (2000), argmax map and grain volumes device->host.
+
+The same line also carries, on one GPU: the FP16- and BF16-storage steps on the
+same workload ("mixed vs FP32"), the errors of FP32/FP16/BF16 storage against
+the FP64 oracle (64^3 case, 1000 steps, fixture tests/golden/fp64_qoi.npz), the
+served stream (sims/hr, p50/p99 time-to-result, capacity, per-result errors of
+the 48^3 requests against FP64-oracle fixtures), the reference's own
+APTsetBC3D + APTrhs_psi kernels compiled for sm_100a timed on the same state,
+and the host-CPU baseline.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cupf|reference]
 Under torchrun each rank runs an independent replica (the step does not shard:
@@ -39,7 +50,8 @@ SERVE_STEPS = 1000  # steps of each served request (the served-stream configurat
 METRIC = "3D APT Mcell-upd/s"
 UNIT = "Mcell-upd/s"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
-TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "apt_step_c2_ncu.md")
+FP64_QOI = os.path.join(ROOT, "tests", "golden", "fp64_qoi.npz")
+ERROR_TOL = 1e-3  # relative error bound on volume fractions and interface position
 
 
 def workload_config(extra=None):
@@ -47,6 +59,7 @@ def workload_config(extra=None):
                      % (*INTERIOR, NUM_PF, GRAINS),
          "interior": list(INTERIOR), "num_pf": NUM_PF, "grains": GRAINS, "seed": SEED,
          "bc": "110", "thermal": "line G=1 K/um R=0.05 m/s", "config_steps": CONFIG_STEPS,
+         "sweep": "every work item computed",
          "l2": "inputs larger than L2 (2 x 2.2 GB pair buffers), no flush"}
     if extra:
         c.update(extra)
@@ -56,22 +69,43 @@ def workload_config(extra=None):
 from cupf_b200.replicas import dist_env, max_over_ranks, replica_throughput  # noqa: E402
 
 
+def physical_gpu(device):
+    """nvidia-smi's name for CUDA device `device`: its UUID (nvidia-smi numbers
+    GPUs in its own order and ignores CUDA_VISIBLE_DEVICES, so an ordinal would
+    name another GPU when the job is pinned to a subset)."""
+    try:
+        import torch
+        u = str(torch.cuda.get_device_properties(device).uuid)
+        if u:
+            return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        pass
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    if vis:
+        ent = [v.strip() for v in vis.split(",") if v.strip()]
+        if device < len(ent):
+            return ent[device]
+    return str(device)
+
+
 class ClockSampler:
-    """nvidia-smi clock/throttle sampling during the timed region."""
+    """nvidia-smi clock/throttle sampling of one GPU during the timed region.
+    `device` is a CUDA ordinal; the sampler resolves it to the physical GPU."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device):
-        self.device = device
+        self.gpu = physical_gpu(device)
         self.proc = None
-        self.path = os.path.join("/tmp", "cupf_clocks_%d_%d.csv" % (os.getpid(), device))
+        self.path = os.path.join("/tmp", "cupf_clocks_%d_%d_%d.csv" % (os.getpid(), device,
+                                                                     time.monotonic_ns()))
 
     def __enter__(self):
         try:
             self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu, "--query-gpu=" + self.Q,
                                           "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
@@ -90,14 +124,15 @@ class ClockSampler:
 
     def summary(self):
         if not self.proc or not os.path.exists(self.path):
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"],
+                    "gpu": self.gpu}
         rows = []
         for line in open(self.path):
             parts = [x.strip() for x in line.split(",")]
             if len(parts) >= 9:
                 rows.append(parts)
         if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "gpu": self.gpu}
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -105,7 +140,7 @@ class ClockSampler:
         load = [v for v in sm if mx and v > 0.3 * max(mx)] or sm
         return {"sm_mhz": float(np.median(load)) if load else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(rows), "gpu": self.gpu, "nvidia_smi_index": rows[0][0]}
 
 
 def measured_peak():
@@ -116,82 +151,79 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per launch of the step kernel from the committed ncu summary."""
-    try:
-        for line in open(TRAFFIC_PROFILE):
-            if line.startswith("traffic_bytes_per_launch_c2:"):
-                return float(line.split(":")[1])
-    except Exception:
-        pass
-    return None
-
-
 def make_case():
     from cupf_b200 import cases
     return cases.line_case(*INTERIOR, num_pf=NUM_PF, num_grains=GRAINS, seed=SEED, bc="110")
 
 
+class _Fp64Stepper:
+    """The FP64 oracle (the reference's step in double precision, OpenMP over all
+    host threads) advancing one state of a case: the CPU side of the comparison."""
+
+    def __init__(self, case):
+        from oracle import CpuOracle
+        self.o = CpuOracle()
+        self.case = case
+        ph32, ids = case.initial_slots()
+        self.ph = ph32.astype(np.float64)
+        del ph32
+        self.ids = ids
+        self.ph_b, self.ids_b = self.ph.copy(), ids.copy()
+        self.n = 0
+
+    def step(self):
+        p = self.case.params
+        self.n += 1
+        t = float(np.float32(np.float32(self.n) * np.float32(p.dt)) * np.float32(p.tau0))
+        self.o.set_bc(p, self.ph, self.ids)
+        self.o.rhs_psi_f64(self.case, t, self.ph, self.ids, self.ph_b, self.ids_b)
+        self.ph, self.ph_b = self.ph_b, self.ph
+        self.ids, self.ids_b = self.ids_b, self.ids
+
+
 def cpu_baseline(case, budget_s=15.0, max_steps=4):
-    """FP64 oracle (OpenMP, all host threads) on the same workload: bounded number of steps."""
-    from oracle import CpuOracle
-    o = CpuOracle()
-    ph32, ids = case.initial_slots()
-    ph = ph32.astype(np.float64)
-    ph_b, ids_b = ph.copy(), ids.copy()
+    """FP64 oracle (OpenMP, all host threads) on the same workload: a bounded
+    number of whole-grid steps from the initial state."""
+    st = _Fp64Stepper(case)
     p = case.params
     cells = (p.fnx - 2) * (p.fny - 2) * (p.fnz - 2)
     steps, t_total = 0, 0.0
     while steps < max_steps and t_total < budget_s:
-        t = float(np.float32(np.float32(steps + 1) * np.float32(p.dt)) * np.float32(p.tau0))
         t0 = time.perf_counter()
-        o.set_bc(p, ph, ids)
-        o.rhs_psi_f64(case, t, ph, ids, ph_b, ids_b)
+        st.step()
         t_total += time.perf_counter() - t0
-        ph, ph_b = ph_b, ph
-        ids, ids_b = ids_b, ids
         steps += 1
-    cores = os.cpu_count()
-    return {"value": cells * steps / t_total / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
+    return {"value": cells * steps / t_total / 1e6, "unit": UNIT, "cores": os.cpu_count(),
+            "kind": "port",
             "sample": "%d FP64 steps of the full %dx%dx%d grid (%.1f s)" % (steps, *INTERIOR, t_total)}
 
 
 def run_reference(args, ws, rank):
     """Reference arm: the reference's algorithm on the host cores (the oracle
-    port in double precision, OpenMP), each step a bounded slab of the workload."""
+    port in double precision, OpenMP over all host threads; the reference ships
+    its step only as CUDA) on the same 256x256x512 grid as the library's arm:
+    `warmup` untimed whole-grid steps, then `steps` timed whole-grid steps from
+    the same initial state."""
     if rank != 0:
         return 0
-    from cupf_b200 import cases
-    from oracle import CpuOracle
-    slab = (INTERIOR[0], INTERIOR[1], 64)
-    c = cases.line_case(*slab, num_pf=NUM_PF, num_grains=GRAINS, seed=SEED, bc="110")
-    o = CpuOracle()
-    ph32, ids = c.initial_slots()
-    ph = ph32.astype(np.float64)
-    ph_b, ids_b = ph.copy(), ids.copy()
-    p = c.params
+    case = make_case()
+    st = _Fp64Stepper(case)
+    p = case.params
     cells = (p.fnx - 2) * (p.fny - 2) * (p.fnz - 2)
-
-    def one(n):
-        nonlocal ph, ph_b, ids, ids_b
-        t = float(np.float32(np.float32(n) * np.float32(p.dt)) * np.float32(p.tau0))
-        o.set_bc(p, ph, ids)
-        o.rhs_psi_f64(c, t, ph, ids, ph_b, ids_b)
-        ph, ph_b = ph_b, ph
-        ids, ids_b = ids_b, ids
-
-    for n in range(args.warmup):
-        one(n + 1)
+    for _ in range(args.warmup):
+        st.step()
     t0 = time.perf_counter()
-    for n in range(args.steps):
-        one(args.warmup + n + 1)
+    for _ in range(args.steps):
+        st.step()
     dt = time.perf_counter() - t0
     v = cells * args.steps / dt / 1e6
-    sample = "each step: one FP64 step of a %dx%dx%d slab of the workload" % slab
+    sample = ("steps %d-%d of the whole %dx%dx%d grid in FP64 (the library arm's grid, state "
+              "and steps)" % (args.warmup + 1, args.warmup + args.steps, *INTERIOR))
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": workload_config({"reference_sample": sample}),
+            "data": "synthetic", "same_config": True,
+            "config": workload_config({"reference_sample": sample}),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                              "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -199,92 +231,138 @@ def run_reference(args, ws, rank):
     return 0
 
 
-SERVE_GRIDS = [(48, 48, 48), (96, 96, 96), (128, 128, 256), (192, 192, 192)]
+def load_fp64_fixture():
+    try:
+        return dict(np.load(FP64_QOI))
+    except Exception:
+        return None
 
 
-def serve_requests(n, seed=0):
-    """Seeded config-4 stream: grid uniform from SERVE_GRIDS, 10-300 grains,
-    seed 0-9999, G 0.1-10 K/um (1e5-1e7 K/m), R 0.01-0.5 m/s, 1000 steps,
-    Poisson arrivals at 4 per second."""
+def qoi_errors(volumes, qoi, ref_volumes, ref_qoi):
+    """Errors of a result against the FP64 oracle: volume-weighted L1 relative
+    error of the grain volume fractions, relative error of the mean interface
+    height (interface position) and of the interface area."""
+    v = np.asarray(volumes, np.float64)
+    r = np.asarray(ref_volumes, np.float64)
+    return {"volume_fraction_l1_rel_err": float(np.abs(v - r).sum() / r.sum()),
+            "interface_height_rel_err": float(abs(qoi[2] - ref_qoi[2]) / ref_qoi[2]),
+            "interface_area_rel_err": float(abs(qoi[1] - ref_qoi[1]) / ref_qoi[1])}
+
+
+def storage_errors(fix, precisions=("fp32", "fp16", "bf16")):
+    """Each storage on the 64^3 line case (20 grains, NUM_PF = 5, 1000 steps,
+    from init_from_argmax like every production path) against the FP64 oracle's
+    QoIs of the same case (tests/golden/fp64_qoi.npz)."""
     from cupf_b200 import cases
-    rng = np.random.default_rng(seed)
-    t = 0.0
-    out = []
-    for _ in range(n):
-        t += rng.exponential(1.0 / 4.0)
-        g = SERVE_GRIDS[rng.integers(len(SERVE_GRIDS))]
-        c = cases.line_case(*g, num_pf=NUM_PF, num_grains=int(rng.integers(10, 301)),
-                            seed=int(rng.integers(0, 10000)), G=float(rng.uniform(0.1, 10.0)),
-                            R=float(rng.uniform(0.01, 0.5)), bc="110")
-        out.append((t, c))
+    from cupf_b200.solver import APTSolver
+    if fix is None:
+        return {"unavailable": "fixture %s missing" % FP64_QOI}
+    c = cases.line_case(64, 64, 64, num_pf=5, num_grains=20, seed=0, bc="110")
+    steps = int(fix["steps"])
+    out = {"case": "64^3 line, 20 grains, NUM_PF=5, %d steps" % steps, "tolerance": ERROR_TOL}
+    for prec in precisions:
+        with APTSolver(c, precision=prec) as s:
+            s.init_from_argmax(c.phi, c.alpha)
+            s.step(steps)
+            s.collect(clear=True)
+            vols = s.grain_volumes(c.params.num_theta)[1:]
+            q = s.qoi_sums()
+        e = qoi_errors(vols, q, fix["c1_volumes"], fix["c1_qoi"])
+        e["within_tolerance"] = bool(e["volume_fraction_l1_rel_err"] <= ERROR_TOL and
+                                     e["interface_height_rel_err"] <= ERROR_TOL)
+        out[prec] = e
     return out
 
 
+def serve_stream(prec, nreq, fix=None, device=0):
+    """Continuous-batching run of the seeded Poisson stream: submit each request
+    at its arrival time, pump the server meanwhile; then the same requests all
+    submitted at once (capacity).  Returns sims/hr, p50/p99 time-to-result,
+    cell-update rates and, for the 48^3 requests, each result's error against
+    the FP64 oracle (fixture)."""
+    from cupf_b200.server import SERVE_GRIDS, Server, poisson_stream
+    reqs = poisson_stream(nreq, seed=0, num_pf=NUM_PF)
+    fix_idx = set(int(i) for i in fix["served_index"]) if fix is not None else set()
+    with Server(device=device, precision=prec, num_pf=NUM_PF, max_active=64, steps_per_round=25,
+                autotune=True) as srv:
+        # warm the autotuner and the kernels on one request of every grid shape
+        shapes = [g for g in SERVE_GRIDS if any(c.meta["interior"] == g for _, c in reqs)]
+        warm = [srv.submit(next(c for _, c in reqs if c.meta["interior"] == g), 5) for g in shapes]
+        srv.run_until_done(warm)
+        for w in warm:
+            srv.release(w)
+        t0 = time.perf_counter()
+        ids = []
+        cells = 0
+        k = 0
+        with ClockSampler(device) as clk:
+            while k < len(reqs) or any(srv.status(r) < 2 for r in ids):
+                now = time.perf_counter() - t0
+                while k < len(reqs) and reqs[k][0] <= now:
+                    c = reqs[k][1]
+                    ids.append(srv.submit(c, SERVE_STEPS))
+                    p = c.params
+                    cells += (p.fnx - 2) * (p.fny - 2) * (p.fnz - 2) * SERVE_STEPS
+                    k += 1
+                running, pending, _ = srv.pump()
+                if running == 0 and pending == 0 and k < len(reqs):
+                    time.sleep(max(0.0, reqs[k][0] - (time.perf_counter() - t0)))
+        res = [srv.result(r) for r in ids]
+        ttr = np.array([r["times"][2] - r["times"][0] for r in res])
+        span = max(r["times"][2] for r in res) - min(r["times"][0] for r in res)
+        errors = []
+        for i, r in enumerate(res):
+            if i in fix_idx:
+                e = qoi_errors(r["volumes"][1:], r["qoi"], fix["srv%d_volumes" % i],
+                               fix["srv%d_qoi" % i])
+                e["request"] = i
+                errors.append(e)
+        for r in ids:
+            srv.release(r)
+        # capacity: the same requests all submitted at once (the paced stream
+        # offers about 12 G cell-updates/s, below what one GPU serves)
+        busy0, _ = srv.stats()
+        with ClockSampler(device) as clk_sat:
+            t1 = time.perf_counter()
+            sat = [srv.submit(c, SERVE_STEPS) for _, c in reqs]
+            srv.run_until_done(sat)
+            sat_span = time.perf_counter() - t1
+        busy = (srv.stats()[0] - busy0) / 1e3
+        for r in sat:
+            srv.release(r)
+    worst = {}
+    if errors:
+        for key in ("volume_fraction_l1_rel_err", "interface_height_rel_err"):
+            worst[key] = max(e[key] for e in errors)
+        worst["within_tolerance"] = bool(all(
+            e["volume_fraction_l1_rel_err"] <= ERROR_TOL and e["interface_height_rel_err"] <= ERROR_TOL
+            for e in errors))
+    return {"precision": prec, "sims_per_hr": len(res) / span * 3600.0,
+            "p50_s": float(np.percentile(ttr, 50)), "p99_s": float(np.percentile(ttr, 99)),
+            "mcell_upd_per_s": cells / span / 1e6, "requests": len(res),
+            "arrival_rate_per_s": 4.0, "steps_per_request": SERVE_STEPS,
+            "capacity": {"sims_per_hr": len(sat) / sat_span * 3600.0,
+                         "mcell_upd_per_s": cells / sat_span / 1e6, "seconds": sat_span,
+                         "device_busy_s": busy, "clocks": clk_sat.summary(),
+                         "note": "the same requests all submitted at once"},
+            "errors_vs_fp64": {"results": errors, "worst": worst, "tolerance": ERROR_TOL,
+                               "which": "every 48^3 request of the stream (the oracle's cost "
+                                        "bounds the rest)"},
+            "clocks": clk.summary()}
+
+
 def run_serve(args):
-    """Continuous-batching benchmark: submit each request at its arrival time,
-    pump the server meanwhile; report sims/hr and p50/p99 time-to-result."""
+    """Continuous-batching benchmark alone: one JSON line per storage."""
     import torch
-    from cupf_b200.server import Server
+    from cupf_b200.server import SERVE_GRIDS
     torch.cuda.set_device(0)
-    reqs = serve_requests(args.serve_requests)
-    lines = []
+    fix = load_fp64_fixture()
     for prec in args.serve_precisions.split(","):
-        with Server(precision=prec, num_pf=NUM_PF, max_active=64, steps_per_round=25,
-                    autotune=True) as srv:
-            # warm the autotuner and the kernels on one request of every grid shape
-            warm = [srv.submit(c, 5) for c in
-                    [next(c for _, c in reqs if c.meta["interior"] == g) for g in SERVE_GRIDS
-                     if any(c.meta["interior"] == g for _, c in reqs)]]
-            srv.run_until_done(warm)
-            for w in warm:
-                srv.release(w)
-            t0 = time.perf_counter()
-            ids = []
-            cells = 0
-            k = 0
-            with ClockSampler(0) as clk:
-                while k < len(reqs) or any(srv.status(r) < 2 for r in ids):
-                    now = time.perf_counter() - t0
-                    while k < len(reqs) and reqs[k][0] <= now:
-                        c = reqs[k][1]
-                        ids.append(srv.submit(c, SERVE_STEPS))
-                        p = c.params
-                        cells += (p.fnx - 2) * (p.fny - 2) * (p.fnz - 2) * SERVE_STEPS
-                        k += 1
-                    running, pending, _ = srv.pump()
-                    if running == 0 and pending == 0 and k < len(reqs):
-                        time.sleep(max(0.0, reqs[k][0] - (time.perf_counter() - t0)))
-            res = [srv.result(r) for r in ids]
-            ttr = np.array([r["times"][2] - r["times"][0] for r in res])
-            span = max(r["times"][2] for r in res) - min(r["times"][0] for r in res)
-            for r in ids:
-                srv.release(r)
-            # capacity: the same requests all submitted at once (the stream above is
-            # paced by its arrivals: 4/s x 1000 steps x 3.1 M cells on average, about
-            # 12 G cell-updates/s of offered load)
-            busy0, _ = srv.stats()
-            with ClockSampler(0) as clk_sat:
-                t1 = time.perf_counter()
-                sat = [srv.submit(c, SERVE_STEPS) for _, c in reqs]
-                srv.run_until_done(sat)
-                sat_span = time.perf_counter() - t1
-            busy = (srv.stats()[0] - busy0) / 1e3
-            for r in sat:
-                srv.release(r)
-            lines.append({"metric": "served sims/hr", "impl": "cupf-serve", "precision": prec,
-                          "value": len(res) / span * 3600.0, "unit": "sims/hr",
-                          "p50_s": float(np.percentile(ttr, 50)),
-                          "p99_s": float(np.percentile(ttr, 99)),
-                          "mcell_upd_per_s": cells / span / 1e6, "requests": len(res),
-                          "arrival_rate_per_s": 4.0, "steps_per_request": SERVE_STEPS,
-                          "saturated": {"sims_per_hr": len(sat) / sat_span * 3600.0,
-                                        "mcell_upd_per_s": cells / sat_span / 1e6,
-                                        "seconds": sat_span, "device_busy_s": busy,
-                                        "clocks": clk_sat.summary(),
-                                        "note": "all requests submitted at once"},
-                          "grids": [list(g) for g in SERVE_GRIDS], "clocks": clk.summary(),
-                          "data": "synthetic Poisson stream, seed 0"})
-            print(json.dumps(lines[-1]), flush=True)
+        r = serve_stream(prec, args.serve_requests, fix)
+        line = {"metric": "served sims/hr", "impl": "cupf-serve", "value": r["sims_per_hr"],
+                "unit": "sims/hr", **r, "grids": [list(g) for g in SERVE_GRIDS],
+                "data": "synthetic Poisson stream, seed 0"}
+        print(json.dumps(line), flush=True)
     return 0
 
 
@@ -532,13 +610,17 @@ def run_dense(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="cupf", choices=["cupf", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--serve", action="store_true", help="served-batch benchmark (config 4)")
-    ap.add_argument("--serve-requests", type=int, default=40)
+    ap.add_argument("--serve-requests", type=int, default=40,
+                    help="requests of the served stream (0: no served run in the default line)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="headline only: no other storages, errors, served stream or reference "
+                         "kernels")
     ap.add_argument("--serve-precisions", default="fp32,fp16")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp16"])
     ap.add_argument("--interior", type=int, nargs=3, metavar=("NX", "NY", "NZ"),
@@ -564,6 +646,43 @@ def main():
     if args.workload == "dense":
         return run_dense(args)
 
+    return run_apt3d(args, ws, rank, local)
+
+
+def reference_kernels(case, steps, warmup):
+    """The reference's own APTsetBC3D + APTrhs_psi pair (3DgrainMPI/APTPhaseField.cu,
+    compiled unmodified for sm_100a; block 32x4 as its evolve loop launches it),
+    timed on the device over the same steps from the same initial state."""
+    import ctypes as C
+    import torch
+    try:
+        from oracle import RefGPU
+        ref = RefGPU(NUM_PF)
+    except (FileNotFoundError, OSError) as e:
+        return {"unavailable": str(e)}
+    p = case.params
+    ref.check(ref.L.ref_set_params(p))
+    ph0, id0 = case.initial_slots()
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    x, y, z, sint, cost = (dev(a) for a in (case.x, case.y, case.z, case.sint, case.cost))
+    a_ph, a_id, b_ph, b_id = dev(ph0), dev(id0), dev(ph0), dev(id0)
+    del ph0, id0
+    ms = C.c_float()
+    args = [x.data_ptr(), y.data_ptr(), z.data_ptr(), a_ph.data_ptr(), b_ph.data_ptr(),
+            a_id.data_ptr(), b_id.data_ptr(), sint.data_ptr(), cost.data_ptr()]
+    w = warmup + (warmup % 2)  # the harness runs step pairs; an even warm-up keeps the buffers
+    ref.check(ref.L.ref_run_steps(w, 0, *args, C.byref(ms)))
+    ref.check(ref.L.ref_run_steps(steps, w, *args, C.byref(ms)))
+    del a_ph, a_id, b_ph, b_id
+    torch.cuda.empty_cache()
+    cells = (p.fnx - 2) * (p.fny - 2) * (p.fnz - 2)
+    return {"ms_per_step": ms.value / steps, "value": cells * steps / ms.value / 1e3,
+            "unit": UNIT, "steps": steps, "warmup": w,
+            "what": "reference APTsetBC3D + APTrhs_psi (3DgrainMPI/APTPhaseField.cu) compiled "
+                    "for sm_100a, same grid and initial state, device time"}
+
+
+def run_apt3d(args, ws, rank, local):
     import torch
     from cupf_b200.solver import APTSolver
     pg = None
@@ -575,65 +694,96 @@ def main():
         pg = dist
     device = local if ws > 1 else 0
     torch.cuda.set_device(device)
+    extras = ws == 1 and not args.no_extras
 
     case = make_case()
     p = case.params
     cells = (p.fnx - 2) * (p.fny - 2) * (p.fnz - 2)
-    solver = APTSolver(case, precision=args.precision, device=device)
-    solver.init_from_argmax(case.phi, case.alpha)
-    solver.step(args.warmup)
-    solver.sync()
 
     def barrier():
         if pg:
             pg.barrier()
         torch.cuda.synchronize(device)
 
-    barrier()
-    solver.active_cells()  # restart the counter of computed cells
-    with ClockSampler(device) as clk:
+    def window(solver, skip_quiet, clocks=False):
+        """From the initial state: `warmup` untimed steps, then `steps` timed steps
+        (CUDA events on the solver's stream, max over ranks)."""
+        solver.init_from_argmax(case.phi, case.alpha)
+        solver.set_skip_quiet(skip_quiet)
+        solver.step(args.warmup)
+        barrier()
+        solver.active_cells()  # restart the counter of computed cells
+        clk = ClockSampler(device) if clocks else None
+        if clk:
+            clk.__enter__()
         ms = solver.time_steps(args.steps)
-    barrier()
-    active = solver.active_cells() / args.steps  # cells of the computed items per launch
-    ms = max_over_ranks(pg, ms, "cuda")
+        if clk:
+            # keep the GPU under the same load for about half a second more, so the
+            # sampler (100 ms period) sees the clocks of this kernel even when the
+            # timed region itself is shorter than its period
+            t_end = time.perf_counter() + 0.5
+            while time.perf_counter() < t_end:
+                solver.step(max(1, args.steps))
+                solver.sync()
+            clk.__exit__(None, None, None)
+        barrier()
+        active = solver.active_cells() / args.steps  # cells of the computed items per launch
+        ms = max_over_ranks(pg, ms, "cuda")
+        return ms, active, clk.summary() if clk else None
+
+    bytes_per_cell = {"fp32": 16, "fp16": 8, "bf16": 8}
+    with APTSolver(case, precision=args.precision, device=device) as solver:
+        ms, active, clocks = window(solver, False, clocks=True)
+        ms_q, active_q, _ = window(solver, True)
     value = replica_throughput(ws, cells, args.steps, ms)
-
-    # The same number of steps with every work item computed (the reference's full
-    # sweep, no quiet items left alone), continuing from the state reached above.
-    solver.set_skip_quiet(False)
-    solver.step(2)
-    barrier()
-    ms_full = max_over_ranks(pg, solver.time_steps(args.steps), "cuda")
-    solver.set_skip_quiet(True)
-
-    # roofline of the step kernel (the only kernel in the timed region): the
-    # algorithmic bytes are the slot pairs of the cells it computes, each read
-    # once and written once; the cells of quiet items are neither read nor written
-    bytes_per_cell = 2 * NUM_PF * (8 if args.precision == "fp32" else 4)
+    bpc = NUM_PF * bytes_per_cell[args.precision]
     launch_s = ms / 1e3 / args.steps
-    achieved = active * bytes_per_cell / launch_s / 1e9
+    achieved = cells * bpc / launch_s / 1e9
     peak, peak_kind = measured_peak()
-    traffic = profile_traffic()
+    # roofline of the step kernel (the only kernel in the timed region): every
+    # interior cell's slot pairs read once and written once.  DRAM traffic is not
+    # measured by this run (a profiler capture is needed): null here.
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic,
+                "frac": achieved / peak, "traffic": None,
                 "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
-                "algorithmic_bytes_per_launch": active * bytes_per_cell,
-                "computed_cells_per_launch": active, "interior_cells": cells}
-    full_sweep = {"value": replica_throughput(ws, cells, args.steps, ms_full), "unit": UNIT,
-                  "ms_per_step": ms_full / args.steps,
-                  "hbm_gbs": cells * bytes_per_cell / (ms_full / 1e3 / args.steps) / 1e9,
-                  "note": "every work item computed, steps %d-%d" % (
-                      args.warmup + args.steps + 3, args.warmup + 2 * args.steps + 2)}
+                "algorithmic_bytes_per_launch": cells * bpc,
+                "algorithmic_bytes_per_cell": bpc, "interior_cells": cells}
+    quiet = {"value": replica_throughput(ws, cells, args.steps, ms_q), "unit": UNIT,
+             "ms_per_step": ms_q / args.steps, "computed_cells_per_launch": active_q,
+             "computed_hbm_gbs": active_q * bpc / (ms_q / 1e3 / args.steps) / 1e9,
+             "note": "same state and steps; work items whose cells stay exact empty pairs are "
+                     "left alone (results bit-identical); value counts every interior cell"}
+
+    # the other storages on the same workload (mixed vs FP32)
+    precisions = None
+    if extras:
+        precisions = {args.precision: {"value": value, "ms_per_step": ms / args.steps,
+                                       "hbm_gbs": achieved, "quiet_skip_value": quiet["value"]}}
+        for prec in ("fp16", "bf16"):
+            if prec == args.precision:
+                continue
+            with APTSolver(case, precision=prec, device=device) as s2:
+                m2, _, _ = window(s2, False)
+                m2q, _, _ = window(s2, True)
+            bpc2 = NUM_PF * bytes_per_cell[prec]
+            precisions[prec] = {"value": cells * args.steps / m2 / 1e3,
+                                "ms_per_step": m2 / args.steps,
+                                "hbm_gbs": cells * bpc2 / (m2 / 1e3 / args.steps) / 1e9,
+                                "quiet_skip_value": cells * args.steps / m2q / 1e3,
+                                "speedup_vs_fp32_full_sweep": ms / m2}
+        fix = load_fp64_fixture()
+        precisions["errors_vs_fp64"] = storage_errors(fix)
 
     # end to end through the C ABI with host buffers: a whole C2 simulation
     e2e = None
     if not args.no_e2e:
-        def through_abi(nsteps):
+        def through_abi(nsteps, skip_quiet):
             """create + H2D of phi/alpha + nsteps + argmax D2H + volumes, host wall time
             (max over ranks)."""
             barrier()
             t0 = time.perf_counter()
             with APTSolver(case, precision=args.precision, device=device) as s2:
+                s2.set_skip_quiet(skip_quiet)
                 s2.init_from_argmax(case.phi, case.alpha)
                 s2.step(nsteps)
                 phi, alpha = s2.collect(clear=True)
@@ -644,21 +794,34 @@ def main():
             return sec
 
         L = case.length
-        # a whole C2 simulation (2000 steps) through the C ABI: the configuration's
-        # own workload, and the headline end-to-end number
-        full_s = through_abi(CONFIG_STEPS)
-        # and the same steps as the device-timed region (warm-up + timed steps from
-        # the same initial state): the state is young there, with more active slots
-        # per cell than the simulation's average, and the fixed costs weigh more
-        nwin = args.warmup + args.steps
-        win_s = through_abi(nwin)
+        full_s = through_abi(CONFIG_STEPS, False)
+        quiet_s = through_abi(CONFIG_STEPS, True)
         e2e = {"value": ws * cells * CONFIG_STEPS / full_s / 1e6, "unit": UNIT,
                "h2d_bytes_per_step": (8 * L) / CONFIG_STEPS,  # phi + alpha, float32/int32
                "d2h_bytes_per_step": (8 * L + 8 * (GRAINS + 1)) / CONFIG_STEPS,
                "steps": CONFIG_STEPS, "seconds": full_s,
-               "includes": "handle create + H2D phi/alpha + 2000 steps + argmax D2H + volumes",
-               "same_steps_as_timed_region": {"value": ws * cells * nwin / win_s / 1e6,
-                                              "steps": nwin, "seconds": win_s}}
+               "includes": "handle create + H2D phi/alpha + 2000 steps (every work item "
+                           "computed) + argmax D2H + volumes",
+               "quiet_skip": {"value": ws * cells * CONFIG_STEPS / quiet_s / 1e6,
+                              "seconds": quiet_s}}
+
+    served = None
+    ref_k = None
+    if extras:
+        ref_k = reference_kernels(case, args.steps, args.warmup)
+        if "ms_per_step" in ref_k:
+            ref_k["speedup_full_sweep"] = ref_k["ms_per_step"] / (ms / args.steps)
+        if args.serve_requests > 0:
+            fix = load_fp64_fixture()
+            served = {}
+            for prec in args.serve_precisions.split(","):
+                served[prec] = serve_stream(prec, args.serve_requests, fix, device)
+            if "fp32" in served:
+                fp32_single = cells * args.steps / (ms if args.precision == "fp32" else
+                                                    precisions["fp32"]["ms_per_step"] * args.steps) / 1e3
+                for prec, r in served.items():
+                    r["capacity_vs_fp32_single_full_sweep"] = (r["capacity"]["mcell_upd_per_s"] /
+                                                               fp32_single)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -671,18 +834,14 @@ def main():
                 "dtype": "fp32" if args.precision == "fp32" else args.precision + " storage, fp32 compute",
                 "data": "synthetic",
                 "config": workload_config({"parallelism": "replicas x%d" % ws,
-                                           "storage": args.precision,
-                                           "quiet_items": "work items whose cells stay exact "
-                                           "empty pairs are left alone (results bit-identical "
-                                           "to the full sweep, which full_sweep times); "
-                                           "computed cells per launch %d of %d" % (active, cells)}),
+                                           "storage": args.precision}),
                 "hbm_gbs": achieved, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "full_sweep": full_sweep,
-                "clocks": clk.summary(), "gpu_launches": args.steps,
+                "quiet_skip": quiet, "precisions": precisions, "served": served,
+                "reference_kernels": ref_k,
+                "clocks": clocks, "gpu_launches": args.steps,
                 "baseline_metric": "3D APT Mcell-upd/s & HBM GB/s, mixed vs FP32; served sims/hr,"
                                    " p50/p99 at <=1e-3 err"}
         print(json.dumps(line), flush=True)
-    solver.close()
     if pg:
         pg.barrier()
         pg.destroy_process_group()

@@ -12,6 +12,30 @@ _IP = C.POINTER(C.c_int32)
 
 PENDING, RUNNING, DONE, FAILED = 0, 1, 2, 3
 
+# Grid shapes of the served request stream (interior cells).
+SERVE_GRIDS = [(48, 48, 48), (96, 96, 96), (128, 128, 256), (192, 192, 192)]
+
+
+def poisson_stream(n, seed=0, num_pf=8, rate=4.0):
+    """Seeded stream of 3D grain requests: list of (arrival time in s, Case).
+
+    Arrivals are Poisson at `rate` per second; each request draws its interior
+    grid uniformly from SERVE_GRIDS, 10-300 grains, a substrate seed in 0-9999,
+    G uniform in 0.1-10 K/um (1e5-1e7 K/m) and R uniform in 0.01-0.5 m/s (the
+    time step follows R through the reference's cfl rule)."""
+    from . import cases
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for _ in range(n):
+        t += rng.exponential(1.0 / rate)
+        g = SERVE_GRIDS[rng.integers(len(SERVE_GRIDS))]
+        c = cases.line_case(*g, num_pf=num_pf, num_grains=int(rng.integers(10, 301)),
+                            seed=int(rng.integers(0, 10000)), G=float(rng.uniform(0.1, 10.0)),
+                            R=float(rng.uniform(0.01, 0.5)), bc="110")
+        out.append((t, c))
+    return out
+
 
 class Server:
     def __init__(self, device=0, precision="fp32", num_pf=8, max_active=64, steps_per_round=50,

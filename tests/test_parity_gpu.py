@@ -74,7 +74,9 @@ def test_c1_200_steps_bit_exact(built):
 
 def test_c2_200_steps_bit_exact(built):
     """Configuration C2 (the benchmark workload): 256x256x512 interior, 600 grains,
-    NUM_PF=8, its parity window of 200 steps; then the argmax map of both."""
+    NUM_PF=8, its parity window of 200 steps from set_slots; then the argmax map
+    of both, the library's run entering through init_from_argmax as the
+    benchmark does."""
     import torch
     from cupf_b200.solver import APTSolver
     from oracle import RefGPU
@@ -103,9 +105,11 @@ def test_c2_200_steps_bit_exact(built):
     r_phi, r_alpha = phi.cpu().numpy(), alpha.cpu().numpy()
     del d_ph, d_id, phi, alpha
     torch.cuda.empty_cache()
-    ph0, id0 = c.initial_slots()
+    # the benchmark's own entry: the library initialises the slots from the
+    # argmax field (init_from_argmax) instead of set_slots; the argmax map after
+    # 200 steps must be the reference's
     with APTSolver(c) as s:
-        s.set_slots(ph0, id0, 0)
+        s.init_from_argmax(c.phi, c.alpha)
         s.step(200)
         my_phi, my_alpha = s.collect(clear=True)
     assert np.array_equal(my_alpha[m], r_alpha[m])

@@ -32,14 +32,26 @@ def test_noalloc_volumes_equal_allocating_entry_point(built):
         _, alpha = s.collect(clear=True)
         expected = s.grain_volumes(p.num_theta)
     assert expected[1:].sum() > 0
+    # independent count on the host: ids 1..num_grains over the interior, the
+    # rest in counts[0]
+    a = alpha.reshape(p.fnz, p.fny, p.fnx)[1:-1, 1:-1, 1:-1].ravel()
+    ok = (a >= 1) & (a <= p.num_theta)
+    host = np.bincount(a[ok], minlength=p.num_theta + 1).astype(np.int64)
+    host[0] = int(np.count_nonzero(~ok))
+    assert np.array_equal(expected, host)
     d_alpha = torch.from_numpy(np.ascontiguousarray(alpha)).cuda()
+    torch.cuda.synchronize()
     L = abi.lib()
+    free = []
     for call in range(2):
         counts = np.full(p.num_theta + 1, -7, np.int64)
         abi.check(L.cupf_grain_volumes_noalloc(C.c_void_p(d_alpha.data_ptr()), p.fnx, p.fny,
                                                p.fnz, p.num_theta,
                                                counts.ctypes.data_as(C.POINTER(C.c_int64)), None))
+        free.append(torch.cuda.mem_get_info()[0])
         assert np.array_equal(counts, expected), "call %d" % call
+    # the second call allocates nothing: free device memory is unchanged
+    assert free[0] == free[1], free
     # beyond the fixed scratch: rejected with a clear error, nothing launched
     counts = np.zeros(2, np.int64)
     st = L.cupf_grain_volumes_noalloc(C.c_void_p(d_alpha.data_ptr()), p.fnx, p.fny, p.fnz,
