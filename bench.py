@@ -18,7 +18,7 @@ the configuration (2000), argmax map and grain volumes device->host.
 
 The same line also carries, on one GPU: the FP16- and BF16-storage steps on the
 same workload ("mixed vs FP32"), the errors of FP32/FP16/BF16 storage against
-the FP64 oracle (64^3 case, 1000 steps, fixture tests/golden/fp64_qoi.npz), the
+the FP64 oracle (64^3 case, 1000 steps, fixture tests/golden/fp64/qoi.npz), the
 served stream (sims/hr, p50/p99 time-to-result, capacity, per-result errors of
 the 48^3 requests against FP64-oracle fixtures), the reference's own
 APTsetBC3D + APTrhs_psi kernels compiled for sm_100a timed on the same state,
@@ -50,7 +50,7 @@ SERVE_STEPS = 1000  # steps of each served request (the served-stream configurat
 METRIC = "3D APT Mcell-upd/s"
 UNIT = "Mcell-upd/s"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
-FP64_QOI = os.path.join(ROOT, "tests", "golden", "fp64_qoi.npz")
+FP64_QOI = os.path.join(ROOT, "tests", "golden", "fp64", "qoi.npz")
 ERROR_TOL = 1e-3  # relative error bound on volume fractions and interface position
 
 
@@ -252,7 +252,7 @@ def qoi_errors(volumes, qoi, ref_volumes, ref_qoi):
 def storage_errors(fix, precisions=("fp32", "fp16", "bf16")):
     """Each storage on the 64^3 line case (20 grains, NUM_PF = 5, 1000 steps,
     from init_from_argmax like every production path) against the FP64 oracle's
-    QoIs of the same case (tests/golden/fp64_qoi.npz)."""
+    QoIs of the same case (tests/golden/fp64/qoi.npz)."""
     from cupf_b200 import cases
     from cupf_b200.solver import APTSolver
     if fix is None:

@@ -1,7 +1,7 @@
 """Generate the FP64 QoIs that split-precision and served results are measured
 against (CPU only; the oracle's FP64 transcription of the reference step).
 
-Writes tests/golden/fp64_qoi.npz with, for each case, the per-grain voxel
+Writes tests/golden/fp64/qoi.npz with, for each case, the per-grain voxel
 counts of the argmax map after the case's steps (interior cells, ids 1..NG) and
 the FP64 (solid volume, interface area, mean interface height):
 
@@ -58,4 +58,4 @@ def main(out):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden", "fp64_qoi.npz"))
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden", "fp64", "qoi.npz"))
