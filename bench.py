@@ -268,6 +268,9 @@ def storage_errors(fix, precisions=("fp32", "fp16", "bf16")):
             vols = s.grain_volumes(c.params.num_theta)[1:]
             q = s.qoi_sums()
         e = qoi_errors(vols, q, fix["c1_volumes"], fix["c1_qoi"])
+        if "c1_f32_volumes" in fix:
+            e["fp32_oracle"] = qoi_errors(fix["c1_f32_volumes"], fix["c1_f32_qoi"],
+                                          fix["c1_volumes"], fix["c1_qoi"])
         e["within_tolerance"] = bool(e["volume_fraction_l1_rel_err"] <= ERROR_TOL and
                                      e["interface_height_rel_err"] <= ERROR_TOL)
         out[prec] = e
@@ -316,6 +319,14 @@ def serve_stream(prec, nreq, fix=None, device=0):
                 e = qoi_errors(r["volumes"][1:], r["qoi"], fix["srv%d_volumes" % i],
                                fix["srv%d_qoi" % i])
                 e["request"] = i
+                e["grid"] = list(reqs[i][1].meta["interior"])
+                e["grains"] = reqs[i][1].meta["num_grains"]
+                if "srv%d_f32_volumes" % i in fix:
+                    # what single precision itself (the oracle's FP32 restatement of
+                    # the reference) makes of the same request against FP64
+                    e["fp32_oracle"] = qoi_errors(fix["srv%d_f32_volumes" % i],
+                                                  fix["srv%d_f32_qoi" % i],
+                                                  fix["srv%d_volumes" % i], fix["srv%d_qoi" % i])
                 errors.append(e)
         for r in ids:
             srv.release(r)
