@@ -30,13 +30,13 @@ struct BatchSim {
 template <int NP, class S>
 __global__ void __launch_bounds__(NTHREADS, step_min_blocks<NP, S>())
     apt_batch_step_kernel(BatchSim* sims, const CUtensorMap* tmaps, const int4* items, int nitems,
-                          int* work) {
+                          int* work, const int* err) {
   extern __shared__ __align__(128) unsigned char smem[];
   CtaSmem<NP, S> sm(smem);
   sm.init();
   int qbase = 0;
   for (;;) {
-    const int it = next_work_item(work, nitems, sm.s_item);
+    const int it = next_work_item(work, nitems, sm.s_item, err);
     if (it < 0) break;
     const int4 w = items[it];  // simulation, txi, tyi, zci
     const BatchSim* sd = sims + w.x;

@@ -12,11 +12,13 @@
 // completed on per-stage mbarriers.  Computing plane k needs planes k-1, k, k+1
 // resident; planes k+2, k+3 are in flight.
 //
-// Boundary fill is done on the read side: plane indices 0 and fnz-1 are loaded
-// from their mapped source planes, and halo cells of x/y are overwritten in
-// shared memory from their mapped interior source in global memory.  The halo
-// cells of the pair buffers in HBM are therefore never written by the step; a
-// separate fill kernel materialises them before any read-back.
+// Boundary fill: plane indices 0 and fnz-1 are loaded from their mapped source
+// planes (TMA coordinate remap), and the x/y halo cells are read from HBM,
+// where they hold their mapped interior source: the step writes every cell it
+// computes also into the halo cells that map to it, and every other writer of
+// the pair buffers (initialisation, import, nucleation, domain shift) is
+// followed by a fill of the halo.  Halo edges and corners, which no 7-point
+// stencil reads, are not maintained by the step.
 //
 // After a plane lands, each cell of its tile gets a slot-occupancy bit mask
 // (bit p set when slot p holds an id).  The merge then visits only occupied
@@ -180,7 +182,6 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
   uint64_t* bars = sm.bars;
   int* s_abort = sm.s_abort;
   int* s_issued = sm.s_issued;
-  const P* gin = static_cast<const P*>(a.in);
   P* gout = static_cast<P*>(a.out);
 
   const int tid = threadIdx.x;
@@ -212,32 +213,17 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
     for (int q = 0; q < npre; ++q) issue(q);
   }
 
-  // Wait for plane q, patch its x/y halo cells from their mapped sources, and
-  // compute the occupancy masks of its cells (same thread per cell for both).
+  // Wait for plane q and compute the occupancy masks of its cells.
   auto land = [&](int q) {
     const int g = q0 + q;
     const int s = g % STAGES;
     const uint32_t parity = (uint32_t)((g / STAGES) & 1);
-    if (!*s_abort) {
-      // another CTA already gave up: do not spend a second per CTA finding out again
-      if (*(volatile int*)a.err != 0 || !mbar_wait_bounded(&bars[s], parity)) {
-        atomicCAS(s_abort, 0, g + 1);
-        atomicExch(a.err, ERR_TMA_TIMEOUT);
-      }
+    if (!*s_abort && !mbar_wait_bounded(&bars[s], parity)) {
+      atomicCAS(s_abort, 0, g + 1);
+      atomicExch(a.err, ERR_TMA_TIMEOUT);
     }
-    P* st = stages + (size_t)s * Smem::kStagePairs;
-    const int zl = k_begin - 1 + q;
-    const int zp = bc_map(zl, a.fnz, a.bcZ);
+    const P* st = stages + (size_t)s * Smem::kStagePairs;
     for (int c = tid; c < BCELLS; c += NTHREADS) {
-      const int sx = c % BW, sy = c / BW;
-      const int gx = x0 - 1 + sx, gy = y0 - 1 + sy;
-      const bool inside = gx < a.fnx && gy < a.fny;
-      if (inside && (gx == 0 || gx == a.fnx - 1 || gy == 0 || gy == a.fny - 1)) {
-        const int mx = bc_map(gx, a.fnx, a.bcX), my = bc_map(gy, a.fny, a.bcY);
-        const long long src = (long long)zp * plane_pairs + (long long)my * a.xp + mx;
-#pragma unroll
-        for (int p = 0; p < NP; ++p) st[p * BCELLS + c] = gin[p * ss + src];
-      }
       uint32_t m = 0;
 #pragma unroll
       for (int p = 0; p < NP; ++p) m |= (uint32_t)(S::id(st[p * BCELLS + c]) != -1) << p;
@@ -255,6 +241,13 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
   const int gx = x0 + tx, gy = y0 + ty;
   const bool valid = gx <= a.fnx - 2 && gy <= a.fny - 2;
   const int c = (ty + 1) * BW + (tx + 1);
+  // offsets (in pairs, 0 = none) from this cell to the x/y halo cells whose
+  // boundary map sources it (APTsetBC3D, APTPhaseField.cu:93-174)
+  const int hdx0 = bc_map(0, a.fnx, a.bcX) == gx ? -gx : 0;
+  const int hdx1 = bc_map(a.fnx - 1, a.fnx, a.bcX) == gx ? a.fnx - 1 - gx : 0;
+  const int hdy0 = bc_map(0, a.fny, a.bcY) == gy ? -gy * a.xp : 0;
+  const int hdy1 = bc_map(a.fny - 1, a.fny, a.bcY) == gy ? (a.fny - 1 - gy) * a.xp : 0;
+  const bool halo_any = (hdx0 | hdx1 | hdy0 | hdy1) != 0;
   // the line profile and the liquid-start undercooling depend on z only: one
   // evaluation per plane instead of one per cell
   const bool plane_T = a.use_iuc || a.thermalType == 0 || a.thermalType == 1;
@@ -293,12 +286,23 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
     mk[6] = masks[sU * BCELLS + c];
 
     P* outp = gout + (long long)k * plane_pairs + (long long)gy * a.xp + gx;
+    // write pair v to output slot j of this cell and to the halo cells it sources
+    auto put = [&](int j, P v) {
+      P* o = outp + j * ss;
+      *o = v;
+      if (halo_any) {
+        if (hdx0) o[hdx0] = v;
+        if (hdx1) o[hdx1] = v;
+        if (hdy0) o[hdy0] = v;
+        if (hdy1) o[hdy1] = v;
+      }
+    };
     bool clive = false;
     const uint32_t any = mk[0] | mk[1] | mk[2] | mk[3] | mk[4] | mk[5] | mk[6];
     if (any == 0) {
       const P empty = S::empty();
 #pragma unroll
-      for (int p = 0; p < NP; ++p) outp[p * ss] = empty;
+      for (int p = 0; p < NP; ++p) put(p, empty);
       continue;
     }
 
@@ -462,7 +466,7 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
       // and register footprint measured faster at three CTAs per SM)
 #pragma unroll
       for (int j = 0; j < NP; ++j)
-        if (j >= n) outp[j * ss] = S::empty();
+        if (j >= n) put(j, S::empty());
       if (upd) {
 #pragma unroll 1
         for (int j = 0; j < n; ++j) {
@@ -471,7 +475,7 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
           for (int q = 1; q < NP; ++q) id = (j == q) ? L[q] : id;
           const P v = update_slot(j, id);
           clive |= !S::is_empty(v);
-          outp[j * ss] = v;
+          put(j, v);
         }
       } else {
         clive = true;
@@ -480,11 +484,11 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
 #pragma unroll
       for (int j = 0; j < NP; ++j) {
         if (j >= n) {
-          outp[j * ss] = S::empty();
+          put(j, S::empty());
         } else if (upd) {
           const P v = update_slot(j, L[j]);
           clive |= !S::is_empty(v);
-          outp[j * ss] = v;
+          put(j, v);
         } else {
           clive = true;  // the reference leaves the slot unwritten
         }
@@ -541,10 +545,14 @@ __device__ __forceinline__ bool item_quiet(const StepArgs& a, int txi, int tyi, 
 // Hand the CTA its next work item from the launch's atomic counter (-1 when
 // none is left).  After its last fetch each CTA counts itself done; the last one
 // resets both words, so the next launch (or graph replay) starts from zero.
-__device__ __forceinline__ int next_work_item(int* work, int nitems, int* s_item) {
+__device__ __forceinline__ int next_work_item(int* work, int nitems, int* s_item,
+                                              const int* err) {
   __syncthreads();  // every thread has read the previous index
   if (threadIdx.x == 0) {
     int it = atomicAdd(work, 1);
+    // a CTA that gave up on a load set the error word: take no further items
+    // (read with the ticket, once per item, not per plane)
+    if (*(volatile const int*)err != 0) it = nitems;
     if (it >= nitems) {
       it = -1;
       __threadfence();
@@ -581,7 +589,7 @@ __global__ void __launch_bounds__(NTHREADS, step_min_blocks<NP, S>())
   const int nitems = per_chunk * a.nzc;
   int qbase = 0;
   for (;;) {
-    const int it = next_work_item(a.work, nitems, sm.s_item);
+    const int it = next_work_item(a.work, nitems, sm.s_item, a.err);
     if (it < 0) break;
     const int zci = it / per_chunk;
     const int r = it - zci * per_chunk;

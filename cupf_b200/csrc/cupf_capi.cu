@@ -543,6 +543,8 @@ extern "C" cupf_status cupf_apt_active_cells(cupf_apt_handle* h, uint64_t* cells
   return CUPF_OK;
 }
 
+static cupf_status fill_halo(cupf_apt_handle* h, int b);
+
 extern "C" cupf_status cupf_apt_init_from_argmax(cupf_apt_handle* h, const float* phi,
                                                  const int32_t* alpha) {
   if (!h || !phi || !alpha) return fail(CUPF_ERR_INVALID, "null argument");
@@ -568,6 +570,9 @@ extern "C" cupf_status cupf_apt_init_from_argmax(cupf_apt_handle* h, const float
   LAUNCH_S(h, init_kernel, grid_for(L), 256, B<S>(h->buf[0]), B<S>(h->buf[1]), h->phi_m,
            h->alpha_m, h->g);
   CK(cudaGetLastError());
+  // the step reads x/y halo cells from the buffer it advances
+  for (int b = 0; b < 2; ++b)
+    if (cupf_status st = fill_halo(h, b)) return st;
   if (cupf_status st = invalidate_quiet(h)) return st;
   h->cur = 0;
   h->steps_done = 0;
@@ -616,6 +621,8 @@ extern "C" cupf_status cupf_apt_set_slots(cupf_apt_handle* h, const float* ph, c
   LAUNCH_S(h, import_kernel, grid_for(n), 256, B<S>(h->buf[0]), h->xfer_ph, h->xfer_id, h->g);
   LAUNCH_S(h, import_kernel, grid_for(n), 256, B<S>(h->buf[1]), h->xfer_ph, h->xfer_id, h->g);
   CK(cudaGetLastError());
+  for (int b = 0; b < 2; ++b)
+    if ((st = fill_halo(h, b))) return st;
   if ((st = invalidate_quiet(h))) return st;
   h->cur = 0;
   h->steps_done = steps_done;
@@ -901,6 +908,8 @@ extern "C" cupf_status cupf_apt_nucleate(cupf_apt_handle* h, int32_t use_initial
   NuclArgs a = nucl_args(h, use_initial_undercooling);
   LAUNCH_S(h, nucleate_kernel, grid_for(nc), 256, B<S>(h->buf[h->cur]), a);
   CK(cudaGetLastError());
+  // nuclei change cells that source halo cells: refill the halo the step reads
+  if (cupf_status st = fill_halo(h, h->cur)) return st;
   if (total) {
     CK(cudaMemcpyAsync(total, h->nucl_count, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
@@ -981,7 +990,9 @@ extern "C" cupf_status cupf_apt_move_domain(cupf_apt_handle* h, int32_t* tip_fro
                        cudaMemcpyDeviceToDevice, h->stream));
     CK(cudaGetLastError());
   }
+  // both buffers hold the shifted interior: refill the halo of both
   if ((st = fill_halo(h, h->cur))) return st;
+  if (*moved && (st = fill_halo(h, h->cur ^ 1))) return st;
   CK(cudaStreamSynchronize(h->stream));
   return check_err_word(h);
 }

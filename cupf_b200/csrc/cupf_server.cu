@@ -250,6 +250,12 @@ static cupf_status admit(cupf_server* s, Request* r, int slot) {
     init_kernel<S><<<gridn(L), 256, 0, st>>>(static_cast<typename S::T*>(r->buf[0]),
                                              static_cast<typename S::T*>(r->buf[1]), r->dphi,
                                              r->dalpha, r->g);
+    // the step reads x/y halo cells from the buffer: fill them on both
+    const long long nh = 2ll * r->g.fnx * r->g.fny + 2ll * r->g.fnx * (r->g.fnz - 2) +
+                         2ll * (r->g.fny - 2) * (r->g.fnz - 2);
+    for (int b = 0; b < 2; ++b)
+      fill_halo_kernel<S><<<gridn(nh), 256, 0, st>>>(static_cast<typename S::T*>(r->buf[b]), r->g,
+                                                     p.bcX, p.bcY, p.bcZ);
     CK(cudaGetLastError());
     // tensor maps of both buffers
     EncodeTiledFn2 enc = encode_fn();
@@ -454,7 +460,7 @@ static cupf_status rebuild(cupf_server* s) {
     CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));                 \
     for (int k = 0; k < s->cfg.steps_per_round; ++k) {                                       \
       apt_batch_step_kernel<N, S><<<grid, NTHREADS, bytes, s->stream>>>(                     \
-          s->d_sims, s->d_tmaps, s->d_items, s->nitems, s->d_next);                          \
+          s->d_sims, s->d_tmaps, s->d_items, s->nitems, s->d_next, s->d_err);                \
       batch_finish_kernel<<<(nsims + 127) / 128, 128, 0, s->stream>>>(s->d_sims, nsims);     \
     }                                                                                        \
     CK(cudaStreamEndCapture(s->stream, &s->graph));                                          \
