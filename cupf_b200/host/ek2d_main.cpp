@@ -27,7 +27,7 @@
 #include "../../include/cupf_ek2d.h"
 #include "ek2d_host.h"
 #include "host_util.h"
-#include "npz_writer.h"
+#include "array_file.h"
 
 using namespace cupf_host;
 
@@ -118,7 +118,7 @@ int main(int argc, char** argv) {
 
   ek2d_concentration(p, phi, U);
   for (int j = 0; j < fny; ++j) y[j] = (float)(yd[j] - ztip0);
-  NpzWriter w;
+  ArrayFile w;
   w.add("phi", phi);
   w.add("Uc", U);
   w.add("x_coordinates", x);
@@ -127,8 +127,8 @@ int main(int argc, char** argv) {
                            (float)info.shifts};
   w.add("qois_tip_front_spacing_shifts", qv);
   const std::string out = outdir + "/line_nx" + std::to_string(p.nx) + "_ny" + std::to_string(p.ny) +
-                          "_Mt" + std::to_string(p.Mt) + "_seed" + std::to_string(p.seed_val) + ".npz";
+                          "_Mt" + std::to_string(p.Mt) + "_seed" + std::to_string(p.seed_val);
   if (!w.write(out)) return die("cannot write the output file");
-  printf("wrote %s\n", out.c_str());
+  printf("wrote %s%s\n", out.c_str(), w.extension());
   return 0;
 }

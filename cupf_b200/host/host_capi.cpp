@@ -5,6 +5,7 @@
 #include "../../include/cupf_host.h"
 #include "host_util.h"
 #include "phase_field.h"
+#include "h5_writer.h"
 #include "qoi.h"
 
 using namespace cupf_host;
@@ -83,6 +84,22 @@ extern "C" int cupf_host_junctions_3d_cells(int fnx, int fny, int fnz, const int
   const int n = (int)v.size();
   for (int i = 0; i < n && i < cap; ++i) nodes[i] = v[i];
   return n;
+}
+
+extern "C" int cupf_host_h5_write(const char* path, int n, const char* const* names,
+                                  const char* kinds, const int32_t* elem_bytes,
+                                  const int64_t* counts, const void* const* data) {
+  if (!path || n < 0 || (n > 0 && (!names || !kinds || !elem_bytes || !counts || !data))) return -1;
+  H5Writer w;
+  for (int i = 0; i < n; ++i) {
+    const char k = kinds[i];
+    const int e = elem_bytes[i];
+    if (!names[i] || counts[i] < 0 || (counts[i] > 0 && !data[i])) return -1;
+    if (!((k == 'i' && (e == 1 || e == 2 || e == 4 || e == 8)) || (k == 'f' && (e == 4 || e == 8))))
+      return -1;
+    w.add_raw(names[i], k, data[i], (size_t)counts[i], (size_t)e);
+  }
+  return w.write(path) ? 0 : -1;
 }
 
 extern "C" int cupf_host_get_param_float(const char* line, const char* key, float* value) {

@@ -12,7 +12,7 @@
 #include <sstream>
 
 #include "host_util.h"
-#include "npz_writer.h"
+#include "array_file.h"
 
 namespace cupf_host {
 
@@ -398,7 +398,7 @@ bool PhaseField::OutputQoIs() {
   const std::string name = outputBaseName() + "_walltime" + std::to_string(params.walltime) +
                            "_frames" + std::to_string(params.nts) + "_Mt" +
                            std::to_string(params.Mt) + "_rank0";
-  NpzWriter w;
+  ArrayFile w;
   w.add("x_coordinates", x);
   w.add("y_coordinates", y);
   w.add("z_coordinates", z_full);
@@ -411,8 +411,8 @@ bool PhaseField::OutputQoIs() {
   w.add("V", std::vector<float>{params.V});
   for (auto& q : qois->mQoIVectorFloatData) w.add(q.first, q.second);
   for (auto& q : qois->mQoIVectorIntData) w.add(q.first, q.second);
-  const std::string path = ds->outputFolder + "/" + name + ".npz";
-  if (!w.write(path)) return setErr("cannot write " + path);
+  const std::string path = ds->outputFolder + "/" + name;
+  if (!w.write(path)) return setErr("cannot write " + path + w.extension());
   return true;
 }
 
@@ -422,15 +422,15 @@ bool PhaseField::OutputField(int currentStep) {
   const std::string name = outputBaseName() + "_frames" + std::to_string(params.nts) + "_Mt" +
                            std::to_string(params.Mt) + "_rank0_time" +
                            std::to_string(currentStep);
-  NpzWriter w;
+  ArrayFile w;
   w.add("x_coordinates", x);
   w.add("y_coordinates", y);
   w.add("z_coordinates", z_full);
   w.add("angles", mac.theta_arr);
   if (ds->useLineConfig) w.add("alpha", alpha_i_full);
   else w.add("alpha", alpha);
-  const std::string path = ds->outputFolder + "/" + name + ".npz";
-  if (!w.write(path)) return setErr("cannot write " + path);
+  const std::string path = ds->outputFolder + "/" + name;
+  if (!w.write(path)) return setErr("cannot write " + path + w.extension());
   return true;
 }
 

@@ -27,6 +27,8 @@ def _lib():
                                             C.c_char_p, C.c_char_p, C.c_int]
         L.cupf_host_setup.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int,
                                       _IP, _FP, _FP, _IP, C.c_int64, C.c_char_p, C.c_int]
+        L.cupf_host_h5_write.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), C.c_char_p,
+                                         _IP, C.POINTER(C.c_int64), C.POINTER(C.c_void_p)]
         _bound = True
     return L
 
@@ -34,6 +36,25 @@ def _lib():
 def _i(a):
     assert a.dtype == np.int32 and a.flags.c_contiguous
     return a.ctypes.data_as(_IP)
+
+
+def h5_write(path, arrays):
+    """Write {name: 1-D numpy array} (signed integers or float32/float64) as an
+    HDF5 file through the drivers' writer (cupf_host_h5_write)."""
+    names = list(arrays)
+    arrs = [np.ascontiguousarray(arrays[k]).reshape(-1) for k in names]
+    for a in arrs:
+        if a.dtype.kind not in "if" or a.dtype.byteorder == ">":
+            raise TypeError("unsupported dtype %s" % a.dtype)
+    n = len(names)
+    cn = (C.c_char_p * n)(*[k.encode() for k in names])
+    kinds = "".join(a.dtype.kind for a in arrs).encode()
+    elem = np.array([a.dtype.itemsize for a in arrs], np.int32)
+    counts = (C.c_int64 * n)(*[a.size for a in arrs])
+    data = (C.c_void_p * n)(*[a.ctypes.data for a in arrs])
+    r = _lib().cupf_host_h5_write(path.encode(), n, cn, kinds, _i(elem), counts, data)
+    if r != 0:
+        raise IOError("cupf_host_h5_write failed for %s" % path)
 
 
 def grain_volumes(fnx, fny, fnz, alpha, cap=1 << 20):

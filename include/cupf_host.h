@@ -39,6 +39,16 @@ int cupf_host_junctions_3d_cells(int fnx, int fny, int fnz, const int32_t* alpha
                                  const int64_t* cells, int64_t ncells, const uint8_t* distinct,
                                  int32_t* nodes, int cap);
 
+/* h5write_1d of a whole file (3DgrainMPI/PhaseFieldCpu.cpp:584-613, as OutputQoIs /
+ * OutputField use it): writes n 1-D datasets into the root group of a new HDF5
+ * file at path (superblock version 0, contiguous little-endian data).  Dataset
+ * i is named names[i] and holds counts[i] elements of kind kinds[i] ('i' signed
+ * integer of 1, 2, 4 or 8 bytes, 'f' IEEE float of 4 or 8 bytes; elem_bytes[i])
+ * read from data[i].  At most 1024 datasets; a repeated name keeps the last.
+ * Returns 0, or -1 on a bad argument or a failed write. */
+int cupf_host_h5_write(const char* path, int n, const char* const* names, const char* kinds,
+                       const int32_t* elem_bytes, const int64_t* counts, const void* const* data);
+
 /* getParam (helper.cpp:44-74); returns 1 if the key was set. */
 int cupf_host_get_param_float(const char* line, const char* key, float* value);
 int cupf_host_get_param_int(const char* line, const char* key, int32_t* value);

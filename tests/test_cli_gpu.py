@@ -1,6 +1,8 @@
 """The phase_field executable runs a line configuration end to end on a B200:
-forcing folder + input file in, QoI archive out with the reference's dataset
-names (PhaseFieldCpu.cpp:493-519, QOI.cpp:19-34)."""
+forcing folder + input file in, an HDF5 file of QoIs out with the reference's
+dataset names (PhaseFieldCpu.cpp:493-519, QOI.cpp:19-34), read back with the
+tests' own HDF5 reader (tests/h5read.py); CUPF_OUTPUT_FORMAT=npz gives the same
+datasets as a NumPy archive."""
 import os
 import subprocess
 
@@ -8,6 +10,7 @@ import numpy as np
 import pytest
 
 from cupf_b200 import preprocess
+from tests.h5read import H5File
 
 pytestmark = pytest.mark.gpu
 
@@ -21,19 +24,29 @@ def test_phase_field_cli_line_run(tmp_path, built):
                                   R=0.05, z0=0.6, top=0.3, t_end=5e-7)
     preprocess.write_input_file(str(tmp_path / "line.py"), Lx, nts=2, asp_ratio_zx=2.0,
                                 moving_ratio=1.0, num_pf=8)
-    out = tmp_path / "out"
-    out.mkdir()
     exe = os.path.join(ROOT, "cupf_b200", "phase_field")
-    r = subprocess.run([exe, "line.py", "-s", "0", "-b", "110", "-l", "1", "-d", "0", "-o", str(out)],
-                       cwd=tmp_path, capture_output=True, text=True, timeout=600)
-    assert r.returncode == 0, r.stderr + r.stdout
-    files = sorted(os.listdir(out))
-    assert len(files) == 1 and files[0].startswith("lineseed0_") and files[0].endswith(".npz")
-    d = np.load(out / files[0])
-    for key in ("x_coordinates", "y_coordinates", "z_coordinates", "angles", "r0", "z0", "x0",
-                "top", "angle", "V", "fractions", "tip_y", "cross_sec", "extra_area",
-                "total_area", "tip_final", "node_region"):
-        assert key in d.files, key
+    runs = {}
+    for fmt in ("h5", "npz"):
+        out = tmp_path / ("out_" + fmt)
+        out.mkdir()
+        env = dict(os.environ)
+        if fmt == "npz":
+            env["CUPF_OUTPUT_FORMAT"] = "npz"
+        r = subprocess.run([exe, "line.py", "-s", "0", "-b", "110", "-l", "1", "-d", "0", "-o",
+                            str(out)], cwd=tmp_path, capture_output=True, text=True, timeout=600,
+                           env=env)
+        assert r.returncode == 0, r.stderr + r.stdout
+        files = sorted(os.listdir(out))
+        assert len(files) == 1 and files[0].startswith("lineseed0_"), files
+        assert files[0].endswith("." + fmt)
+        runs[fmt] = H5File(str(out / files[0])) if fmt == "h5" else np.load(out / files[0])
+    d, z = runs["h5"], runs["npz"]
+    keys = ("x_coordinates", "y_coordinates", "z_coordinates", "angles", "r0", "z0", "x0",
+            "top", "angle", "V", "fractions", "tip_y", "cross_sec", "extra_area",
+            "total_area", "tip_final", "node_region")
+    assert sorted(d.keys()) == sorted(keys) == sorted(z.files)
+    for key in keys:
+        assert d[key].dtype == z[key].dtype and np.array_equal(d[key], z[key]), key
     assert d["tip_y"].shape == (3,)
     assert d["total_area"].reshape(3, 10)[0].sum() > 0
 
@@ -57,7 +70,7 @@ def _nucleation_run(tmp_path, tag, n_flag, pre_mt):
     assert r.returncode == 0, r.stderr + r.stdout
     files = sorted(os.listdir(out))
     assert len(files) == 1 and "Mixed_density1.000000_grains" in files[0], files
-    return np.load(out / files[0]), files[0]
+    return H5File(str(out / files[0])), files[0]
 
 
 def test_phase_field_cli_liquid_start_nucleation(tmp_path, built):
@@ -73,7 +86,7 @@ def test_phase_field_cli_liquid_start_nucleation(tmp_path, built):
     assert name.split("_grains")[1].startswith(str(len(np.unique(g2p))) + "_")
     d2, name2 = _nucleation_run(tmp_path, "b", 1, 60)
     assert name2 == name
-    for k in d.files:
+    for k in d.keys():
         assert np.array_equal(d[k], d2[k]), k
 
 

@@ -345,9 +345,10 @@ def test_phase_field_cli_full_pf_mode(tmp_path, built):
                         str(out)], cwd=tmp_path, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr + r.stdout
     files = sorted(os.listdir(out))
-    assert len(files) == 1 and files[0].endswith(".npz")
-    d = np.load(out / files[0])
+    assert len(files) == 1 and files[0].endswith(".h5")
+    from tests.h5read import H5File
+    d = H5File(str(out / files[0]))
     for key in ("fractions", "tip_y", "cross_sec", "total_area", "node_region"):
-        assert key in d.files, key
+        assert key in d, key
     assert d["tip_y"].shape == (3,)
     assert d["total_area"].reshape(3, 10)[0].sum() > 0

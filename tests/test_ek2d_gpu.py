@@ -184,7 +184,8 @@ def test_phase_field_2d_executable(built, tmp_path):
     r = subprocess.run([exe, inp, str(tmp_path), "-o", str(tmp_path)], capture_output=True, text=True,
                        timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
-    out = np.load(os.path.join(str(tmp_path), "line_nx64_ny256_Mt300_seed0.npz"))
+    from tests.h5read import H5File
+    out = H5File(os.path.join(str(tmp_path), "line_nx64_ny256_Mt300_seed0.h5"))
     with EK2DSolver(c) as sv:
         sv.set_state(c.psi, c.U)
         sv.prestep()
