@@ -59,6 +59,7 @@ struct StepArgs {
   const uint8_t* quiet_in;
   uint8_t* quiet_out;
   unsigned long long* active_cells;  // cells of the computed items, accumulated (may be NULL)
+  long long wait_limit;  // SM cycles a stage wait may spin before the step gives up
 };
 
 // Boundary map of one coordinate (APTsetBC3D, APTPhaseField.cu:111-112,134-135,157-158):

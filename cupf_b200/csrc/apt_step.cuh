@@ -99,14 +99,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Wait for a stage with a bounded spin: about one second of SM clock, then
-// give up and report (the caller records an error and carries on so that every
-// thread still reaches every barrier).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+// Wait for a stage with a bounded spin: by default about one second of SM
+// clock (kWaitCycles), then give up and report (the caller records an error and
+// carries on so that every thread still reaches every barrier).
+constexpr long long kWaitCycles = 1ll << 31;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
+                                                  long long limit = kWaitCycles) {
   if (mbar_try_wait(bar, parity)) return true;
   long long t0 = clock64();
   while (!mbar_try_wait(bar, parity)) {
-    if (clock64() - t0 > (1ll << 31)) return false;
+    if (clock64() - t0 > limit) return false;
   }
   return true;
 }
@@ -153,7 +155,8 @@ struct CtaSmem {
     __syncthreads();
   }
   // After a timed-out wait no further loads are issued; before the CTA exits
-  // (and its shared memory is reused) wait, again bounded, for those in flight.
+  // (and its shared memory is reused) wait, bounded by the default limit
+  // whatever the launch's own, for those in flight.
   __device__ void drain() {
     __syncthreads();
     if (threadIdx.x == 0 && *s_abort) {
@@ -218,7 +221,7 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
     const int g = q0 + q;
     const int s = g % STAGES;
     const uint32_t parity = (uint32_t)((g / STAGES) & 1);
-    if (!*s_abort && !mbar_wait_bounded(&bars[s], parity)) {
+    if (!*s_abort && !mbar_wait_bounded(&bars[s], parity, a.wait_limit)) {
       atomicCAS(s_abort, 0, g + 1);
       atomicExch(a.err, ERR_TMA_TIMEOUT);
     }

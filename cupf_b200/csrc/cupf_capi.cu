@@ -96,6 +96,7 @@ struct cupf_apt_handle {
   uint8_t* quiet[2] = {nullptr, nullptr};
   size_t quiet_cap = 0;
   bool skip_quiet = true;
+  long long wait_limit = kWaitCycles;  // stage-wait bound of the step kernel (SM cycles)
   bool zc_user = false;  // z chunk fixed by the caller (set_tuning or CUPF_ZC)
   unsigned long long* active_cells = nullptr;
   // read-back scratch (reference layout, num_pf * length), allocated on first use
@@ -297,6 +298,7 @@ static StepArgs step_args(cupf_apt_handle* h, float t, int use_iuc) {
   a.psi_mac = h->psi_mac;
   a.err = h->err;
   a.work = h->work;
+  a.wait_limit = h->wait_limit;
   return a;
 }
 
@@ -525,6 +527,12 @@ extern "C" cupf_status cupf_apt_set_tuning(cupf_apt_handle* h, int32_t z_chunk) 
   return invalidate_quiet(h);
 }
 
+extern "C" cupf_status cupf_apt_set_wait_limit(cupf_apt_handle* h, int64_t cycles) {
+  if (!h || cycles < 0) return fail(CUPF_ERR_INVALID, "bad argument");
+  h->wait_limit = cycles == 0 ? kWaitCycles : cycles;
+  return CUPF_OK;
+}
+
 extern "C" cupf_status cupf_apt_set_skip_quiet(cupf_apt_handle* h, int32_t enable) {
   if (!h) return fail(CUPF_ERR_INVALID, "null handle");
   CK(cudaSetDevice(h->device));
@@ -574,6 +582,7 @@ extern "C" cupf_status cupf_apt_init_from_argmax(cupf_apt_handle* h, const float
   for (int b = 0; b < 2; ++b)
     if (cupf_status st = fill_halo(h, b)) return st;
   if (cupf_status st = invalidate_quiet(h)) return st;
+  CK(cudaMemsetAsync(h->err, 0, sizeof(int), h->stream));  // a new state: no step has failed
   h->cur = 0;
   h->steps_done = 0;
   h->initialised = true;
@@ -624,6 +633,7 @@ extern "C" cupf_status cupf_apt_set_slots(cupf_apt_handle* h, const float* ph, c
   for (int b = 0; b < 2; ++b)
     if ((st = fill_halo(h, b))) return st;
   if ((st = invalidate_quiet(h))) return st;
+  CK(cudaMemsetAsync(h->err, 0, sizeof(int), h->stream));  // a new state: no step has failed
   h->cur = 0;
   h->steps_done = steps_done;
   h->initialised = true;

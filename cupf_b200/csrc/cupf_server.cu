@@ -328,6 +328,7 @@ static cupf_status admit(cupf_server* s, Request* r, int slot) {
   a.Z_mac = r->ddummy;
   a.psi_mac = r->ddummy;
   a.err = s->d_err;
+  a.wait_limit = kWaitCycles;
   bs.buf[0] = r->buf[0];
   bs.buf[1] = r->buf[1];
   bs.quiet[0] = r->dquiet[0];

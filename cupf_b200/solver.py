@@ -154,6 +154,10 @@ class APTSolver:
     def set_tuning(self, z_chunk):
         abi.check(self.L.cupf_apt_set_tuning(self.h, int(z_chunk)))
 
+    def set_wait_limit(self, cycles):
+        """Bound of the step's plane-load waits in SM cycles (0 = default, ~1 s)."""
+        abi.check(self.L.cupf_apt_set_wait_limit(self.h, int(cycles)))
+
     def set_skip_quiet(self, enable):
         """Leave work items whose cells stay all-empty alone (default on)."""
         abi.check(self.L.cupf_apt_set_skip_quiet(self.h, int(bool(enable))))

@@ -298,6 +298,16 @@ cupf_status cupf_apt_set_tuning(cupf_apt_handle* h, int32_t z_chunk);
  * items its nuclei reach, and a domain shift moves the flags with the planes. */
 cupf_status cupf_apt_set_skip_quiet(cupf_apt_handle* h, int32_t enable);
 
+/* Bound of the step kernel's waits for its plane loads, in SM clock cycles (no
+ * counterpart in the reference, which checks no CUDA error).  0 restores the
+ * default of 2^31 cycles (about one second).  A wait that runs out makes the
+ * step stop loading, wait (with the default bound) for the loads in flight,
+ * record an error word and finish; the next synchronising call returns
+ * CUPF_ERR_TIMEOUT, and the state is undefined until init_from_argmax or
+ * set_slots, which clear the error word.  A short bound is meant for tests of
+ * that path. */
+cupf_status cupf_apt_set_wait_limit(cupf_apt_handle* h, int64_t cycles);
+
 /* Cells of the work items the step computed (not left alone as quiet) since the
  * previous call, summed over steps; the counter restarts at 0. */
 cupf_status cupf_apt_active_cells(cupf_apt_handle* h, uint64_t* cells);

@@ -37,8 +37,25 @@ from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-REF_DIR = os.environ.get("CUPF_REFERENCE_DIR", "/root/reference/3DgrainMPI")
-REF2D_DIR = os.environ.get("CUPF_REFERENCE_2D_DIR", "/root/reference/2DdendriteMPI/line_model")
+def _reference_root():
+    """The reference tree: CUPF_REFERENCE_ROOT, else the reference_path recorded
+    in the repository's BASELINE.json (None when neither names a directory)."""
+    root = os.environ.get("CUPF_REFERENCE_ROOT")
+    if not root:
+        try:
+            import json
+            root = json.load(open(os.path.join(ROOT, "BASELINE.json"))).get("reference_path")
+        except Exception:
+            root = None
+    return root if root and os.path.isdir(root) else None
+
+
+_REF_ROOT = _reference_root()
+REF_DIR = os.environ.get("CUPF_REFERENCE_DIR",
+                         os.path.join(_REF_ROOT, "3DgrainMPI") if _REF_ROOT else "")
+REF2D_DIR = os.environ.get("CUPF_REFERENCE_2D_DIR",
+                           os.path.join(_REF_ROOT, "2DdendriteMPI", "line_model") if _REF_ROOT
+                           else "")
 OUT = os.path.join(HERE, "_ref")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CUDA_INC = "/usr/local/cuda/include"
