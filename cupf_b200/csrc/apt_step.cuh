@@ -99,12 +99,33 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
 // Wait for a stage with a bounded spin: by default about one second of SM
 // clock (kWaitCycles), then give up and report (the caller records an error and
-// carries on so that every thread still reaches every barrier).
+// carries on so that every thread still reaches every barrier).  A try_wait may
+// itself suspend the thread for a hardware-chosen interval, so a bound shorter
+// than kShortWait is kept with non-blocking probes only.
 constexpr long long kWaitCycles = 1ll << 31;
+constexpr long long kShortWait = 1ll << 20;
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
                                                   long long limit = kWaitCycles) {
+  if (limit < kShortWait) {
+    const long long t0 = clock64();
+    do {
+      if (mbar_test_wait(bar, parity)) return true;
+    } while (clock64() - t0 <= limit);
+    return false;
+  }
   if (mbar_try_wait(bar, parity)) return true;
   long long t0 = clock64();
   while (!mbar_try_wait(bar, parity)) {

@@ -136,8 +136,8 @@ extern "C" int cupf_host_get_options(int argc, char** argv, int32_t* out, char* 
 namespace {
 class SetupOnly : public PhaseField {
  public:
-  bool cudaSetup() override { return true; }
-  bool evolve() override { return true; }
+  void cudaSetup() override {}
+  void evolve() override {}
 };
 }  // namespace
 
@@ -157,8 +157,13 @@ extern "C" int cupf_host_setup(const char* input_file, const char* folder, int b
   std::string path = input_file;
   // the thermal type is chosen by the input file's name; the file itself may
   // live elsewhere: try the folder's parent when the bare name does not open
-  bool ok = pf.parseInputParams(path) && pf.cpuSetup() && pf.initField();
-  if (!ok) {
+  MPIsetting1D mpi;
+  mpi.domainPartition();
+  pf.SetMPIManager(&mpi);
+  pf.parseInputParams(path);
+  pf.cpuSetup(&mpi);
+  pf.initField();
+  if (pf.failed()) {
     if (err && err_cap > 0) std::strncpy(err, pf.lastError().c_str(), err_cap);
     return -1;
   }
@@ -174,4 +179,56 @@ extern "C" int cupf_host_setup(const char* input_file, const char* folder, int b
     std::memcpy(alpha, pf.alpha.data(), sizeof(int) * pf.length);
   }
   return 0;
+}
+
+extern "C" int cupf_host_setup_state(const char* input_file, const char* folder, int bcX, int bcY,
+                                     int bcZ, int flags, int32_t* dims, float* fparams, float* x,
+                                     float* y, float* z, float* z_full, float* phi, float* psi,
+                                     int32_t* alpha, float* sint, float* cost, int64_t cap,
+                                     char* err, int err_cap) {
+  if (!input_file || !folder || !dims || !fparams) return -1;
+  DesignSettingData ds;
+  ds.inputFile = input_file;
+  ds.useLineConfig = (flags & 1) != 0;
+  ds.pureNucleation = (flags & 2) != 0;
+  ds.includeNucleation = (flags & 4) != 0;
+  ds.bcX = bcX;
+  ds.bcY = bcY;
+  ds.bcZ = bcZ;
+  SetupOnly pf;
+  pf.SetDesignSetting(&ds);
+  pf.mac.folder = folder;
+  MPIsetting1D mpi;
+  mpi.domainPartition();
+  pf.SetMPIManager(&mpi);
+  pf.parseInputParams(input_file);
+  pf.cpuSetup(&mpi);
+  pf.initField();
+  if (pf.failed()) {
+    if (err && err_cap > 0) std::strncpy(err, pf.lastError().c_str(), err_cap);
+    return -1;
+  }
+  const GlobalConstants& p = pf.params;
+  const int32_t d[8] = {pf.fnx, pf.fny, pf.fnz, p.num_theta, p.Mt, p.nts, p.thermalType, pf.fnz_f};
+  std::memcpy(dims, d, sizeof(d));
+  const float f[20] = {p.dt,  p.tau0, p.lamd, p.hi,  p.G,  p.underCoolingRate, p.z0,
+                       p.kin_delta, p.lxd, p.lyd, p.lzd, p.R, p.V, p.top, p.r0, p.x0,
+                       p.cfl, p.underCoolingRate0, p.W0, p.dx};
+  std::memcpy(fparams, f, sizeof(f));
+  if (x) std::memcpy(x, pf.x.data(), sizeof(float) * pf.fnx);
+  if (y) std::memcpy(y, pf.y.data(), sizeof(float) * pf.fny);
+  if (z) std::memcpy(z, pf.z.data(), sizeof(float) * pf.fnz);
+  if (z_full) std::memcpy(z_full, pf.z_full.data(), sizeof(float) * pf.fnz_f);
+  if (pf.length <= cap) {
+    if (phi) std::memcpy(phi, pf.phi.data(), sizeof(float) * pf.length);
+    if (psi && (long long)pf.psi.size() >= pf.length)
+      std::memcpy(psi, pf.psi.data(), sizeof(float) * pf.length);
+    if (alpha) std::memcpy(alpha, pf.alpha.data(), sizeof(int) * pf.length);
+  }
+  const long long nt = 2ll * p.num_theta + 1;
+  if (nt <= cap) {
+    if (sint) std::memcpy(sint, pf.mac.sint.data(), sizeof(float) * nt);
+    if (cost) std::memcpy(cost, pf.mac.cost.data(), sizeof(float) * nt);
+  }
+  return pf.length <= cap ? 0 : 1;
 }

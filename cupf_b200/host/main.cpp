@@ -18,16 +18,23 @@ int main(int argc, char** argv) {
   // -a selects the full (non-APT) solver, one phi field per grain (main.cpp:39-47)
   std::unique_ptr<PhaseField> pf(ds.useAPT ? static_cast<PhaseField*>(new APTPhaseField())
                                            : new PhaseField());
+  MPIsetting1D mpiManager;  // rank 0 of 1: the whole domain on one GPU
+  mpiManager.domainPartition();
   pf->SetDesignSetting(&ds);
+  pf->SetMPIManager(&mpiManager);
   pf->mac.folder = ds.thermalInputFolder + std::to_string(ds.seedValue);
   pf->params.seed_val = ds.seedValue;
-  bool ok = pf->parseInputParams(ds.inputFile) && pf->cpuSetup();
-  if (ok) {
-    if (ds.useLineConfig) pf->qois.reset(new QOILine(pf->qoiGrid()));
-    else pf->qois.reset(new QOI3D(pf->qoiGrid()));
-    ok = pf->initField() && pf->cudaSetup() && pf->evolve() && pf->OutputQoIs();
+  pf->parseInputParams(ds.inputFile);
+  pf->cpuSetup(&mpiManager);
+  if (!pf->failed()) {
+    if (ds.useLineConfig) pf->qois = new QOILine(pf->params);
+    else pf->qois = new QOI3D(pf->params);
   }
-  if (!ok) {
+  pf->initField();
+  pf->cudaSetup();
+  pf->evolve();
+  pf->OutputQoIs();
+  if (pf->failed()) {
     std::fprintf(stderr, "phase_field: %s\n", pf->lastError().c_str());
     return 1;
   }

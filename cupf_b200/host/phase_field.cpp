@@ -74,7 +74,72 @@ void MovingDomain::allocateMovingDomain(int numGrains, int movingDirectionSize) 
 // ------------------------------------------------------------------ PhaseField
 PhaseField::~PhaseField() {
   if (mDense) cupf_dense_destroy(mDense);
+  delete qois;
 }
+
+// The reference-named entry points: each runs its step unless an earlier one failed.
+void PhaseField::parseInputParams(const std::string fileName) {
+  if (!failed()) parseInputImpl(fileName);
+}
+void PhaseField::cpuSetup(MPIsetting* mpiManager) {
+  if (!failed()) cpuSetupImpl(mpiManager);
+}
+void PhaseField::initField() {
+  if (!failed()) initFieldImpl();
+}
+void PhaseField::cudaSetup() {
+  if (!failed()) denseCudaSetup();
+}
+void PhaseField::evolve() {
+  if (!failed()) denseEvolve();
+}
+void PhaseField::OutputQoIs() {
+  if (!failed()) outputQoIsImpl();
+}
+void PhaseField::OutputField(int currentStep) {
+  if (!failed()) outputFieldImpl(currentStep);
+}
+void APTPhaseField::cudaSetup() {
+  if (!failed()) aptCudaSetup();
+}
+void APTPhaseField::evolve() {
+  if (!failed()) aptEvolve();
+}
+
+void MPIsetting::printMPIsetting() const {
+  std::printf("total/x/y/z number of processors: %d/%d/%d/%d\n", numProcessor, numProcessorX,
+              numProcessorY, numProcessorZ);
+  std::printf("rank/x/y/z processor IDs: %d/%d/%d/%d\n", rank, processorIDX, processorIDY,
+              processorIDZ);
+}
+
+// MPIsetting1D/2D::domainPartition (MPIsetting.cpp:33-51) for rank 0 of 1
+void MPIsetting1D::domainPartition() {
+  numProcessorX = numProcessor;
+  numProcessorY = numProcessorZ = 1;
+  processorIDX = rank;
+  processorIDY = processorIDZ = 0;
+}
+
+void MPIsetting2D::domainPartition() {
+  numProcessorX = numProcessor;
+  numProcessorY = numProcessorZ = 1;
+  processorIDX = rank;
+  processorIDY = processorIDZ = 0;
+}
+
+static QoiGrid qoi_grid_of(const GlobalConstants& p) {
+  QoiGrid g;
+  g.fnx = p.fnx;
+  g.fny = p.fny;
+  g.fnz = p.fnz;
+  g.num_theta = p.num_theta;
+  g.nts = p.nts;
+  g.num_nodes = p.num_nodes;
+  return g;
+}
+QOILine::QOILine(const GlobalConstants& params) : QOILine(qoi_grid_of(params)) {}
+QOI3D::QOI3D(const GlobalConstants& params) : QOI3D(qoi_grid_of(params)) {}
 
 bool PhaseField::check(cupf_status st, const char* what) {
   if (st == CUPF_OK) return true;
@@ -93,7 +158,7 @@ QoiGrid PhaseField::qoiGrid() const {
 }
 
 // PhaseField::parseInputParams (PhaseFieldCpu.cpp:17-256)
-bool PhaseField::parseInputParams(const std::string& fileName) {
+bool PhaseField::parseInputImpl(const std::string& fileName) {
   const DesignSettingData* ds = GetSetDesignSetting();
   std::ifstream f(fileName);
   if (!f.good()) return setErr("cannot open input file " + fileName);
@@ -241,7 +306,11 @@ bool PhaseField::parseInputParams(const std::string& fileName) {
 }
 
 // PhaseField::cpuSetup (PhaseFieldCpu.cpp:258-374), single rank
-bool PhaseField::cpuSetup() {
+bool PhaseField::cpuSetupImpl(MPIsetting* mpiManager) {
+  // one process drives the whole domain (the reference splits it into MPI slabs)
+  if (mpiManager && mpiManager->numProcessor != 1)
+    return setErr("one process drives the whole domain: " +
+                  std::to_string(mpiManager->numProcessor) + " ranks given");
   GlobalConstants& p = params;
   if (p.haloWidth != 1) return setErr("haloWidth must be 1");
   const float dxd = p.dx * p.W0;
@@ -277,7 +346,7 @@ bool PhaseField::cpuSetup() {
 }
 
 // PhaseField::initField (PhaseFieldCpu.cpp:377-459)
-bool PhaseField::initField() {
+bool PhaseField::initFieldImpl() {
   GlobalConstants& p = params;
   const DesignSettingData* ds = GetSetDesignSetting();
   for (int i = 0; i < 2 * p.num_theta + 1; i++) {
@@ -381,13 +450,13 @@ std::string PhaseField::outputBaseName() const {
 
 // PhaseField::OutputQoIs (PhaseFieldCpu.cpp:464-520): junction search, then the
 // coordinates, geometry scalars and every QoI vector, one 1-D dataset each.
-bool PhaseField::OutputQoIs() {
+bool PhaseField::outputQoIsImpl() {
   const DesignSettingData* ds = GetSetDesignSetting();
   if (!qois) return setErr("no QoI object");
   const QoiGrid g = qoiGrid();
   std::vector<long long> cells;
   std::vector<unsigned char> distinct;
-  QOI3D* q3 = dynamic_cast<QOI3D*>(qois.get());
+  QOI3D* q3 = dynamic_cast<QOI3D*>(qois);
   if (ds->useLineConfig)
     qois->searchJunctionsOnImage(g, alpha_i_full.data());
   else if (q3 && deviceJunctionCandidates(cells, distinct))
@@ -417,7 +486,7 @@ bool PhaseField::OutputQoIs() {
 }
 
 // PhaseField::OutputField (PhaseFieldCpu.cpp:522-573): the argmax grain map.
-bool PhaseField::OutputField(int currentStep) {
+bool PhaseField::outputFieldImpl(int currentStep) {
   const DesignSettingData* ds = GetSetDesignSetting();
   const std::string name = outputBaseName() + "_frames" + std::to_string(params.nts) + "_Mt" +
                            std::to_string(params.Mt) + "_rank0_time" +
@@ -491,7 +560,7 @@ cupf_apt_params PhaseField::deviceParams() const {
 }
 
 // APTPhaseField::cudaSetup (APTPhaseField.cu:569-637)
-bool APTPhaseField::cudaSetup() {
+bool APTPhaseField::aptCudaSetup() {
   NUM_PF = params.NUM_PF;
   cupf_apt_params d = deviceParams();
   cupf_apt_inputs in;
@@ -572,7 +641,7 @@ bool APTPhaseField::moveDomain(MovingDomain* md) {
 // t = 0 on the freshly emptied state (:776) changes nothing and is not issued.
 // Without -n, preMt is ignored: the reference's liquid-start phase launches
 // add_nucl on the status and generator arrays that only -n allocates (:733-745).
-bool APTPhaseField::evolve() {
+bool APTPhaseField::aptEvolve() {
   const DesignSettingData* ds = GetSetDesignSetting();
   const bool nucl = ds->includeNucleation;
   MovingDomain md;
@@ -625,7 +694,7 @@ bool APTPhaseField::evolve() {
         std::memcpy(alpha_i_full.data() + (size_t)md.move_count * fnx * fny, alpha.data(),
                     sizeof(int) * std::min<long long>(length, full_length - (long long)md.move_count * fnx * fny));
       }
-      if (!OutputField(2 * kt + 2)) return false;
+      if (!outputFieldImpl(2 * kt + 2)) return false;
     }
     if (!check(cupf_apt_step(mHandle, 1, 0), "cupf_apt_step")) return false;
   }
@@ -638,7 +707,7 @@ bool APTPhaseField::evolve() {
 
 // PhaseField::cudaSetup (PhaseField.cu:431-493): the full-PF solver, one phi field
 // per grain (params.NUM_PF = params.num_theta, :440).
-bool PhaseField::cudaSetup() {
+bool PhaseField::denseCudaSetup() {
   params.NUM_PF = params.num_theta;
   NUM_PF = params.NUM_PF;
   cupf_apt_params d = deviceParams();
@@ -657,7 +726,7 @@ bool PhaseField::cudaSetup() {
 // full-PF evolve does both unconditionally).  The reference's last update of the
 // loop (:604) writes a buffer nothing reads afterwards (the final collect_PF at
 // :617 reads the other one), so the loop stops before it.
-bool PhaseField::evolve() {
+bool PhaseField::denseEvolve() {
   const DesignSettingData* ds = GetSetDesignSetting();
   if (ds && ds->includeNucleation) return setErr("the full-PF mode has no nucleation");
   if (!mDense) return setErr("cudaSetup has not run");

@@ -93,27 +93,80 @@ class MovingDomain {
   std::vector<int> loss_area_host;
 };
 
+// Single-process stand-in for the reference's MPI setting (MPIsetting.h:15-62,
+// MPIsetting.cpp:33-51): one process drives the whole domain on one GPU, so
+// every partition is 1 x 1 x 1 and rank 0 of 1.  The constructors accept the
+// reference's communicator argument whatever its type.
+class MPIsetting {
+ public:
+  MPIsetting() = default;
+  template <class Comm>
+  explicit MPIsetting(Comm) {}
+  virtual ~MPIsetting() = default;
+  void printMPIsetting() const;
+  virtual void domainPartition() = 0;
+
+  int rank = 0, numProcessor = 1;
+  int processorIDX = 0, processorIDY = 0, processorIDZ = 0;
+  int numProcessorX = 1, numProcessorY = 1, numProcessorZ = 1;
+  int nxLocal = 0, nyLocal = 0, nzLocal = 0, nzLocalAll = 0;
+  int haloWidth = 1;
+};
+
+class MPIsetting1D : public MPIsetting {
+ public:
+  MPIsetting1D() = default;
+  template <class Comm>
+  explicit MPIsetting1D(Comm c) : MPIsetting(c) {}
+  void domainPartition() override;
+};
+
+class MPIsetting2D : public MPIsetting {
+ public:
+  MPIsetting2D() = default;
+  template <class Comm>
+  explicit MPIsetting2D(Comm c) : MPIsetting(c) {}
+  void domainPartition() override;
+};
+
+// The solver interface of the reference (cuPDE.h:4-21).
+class PDE {
+ public:
+  virtual ~PDE() = default;
+  virtual void cpuSetup(MPIsetting* mpiManager) = 0;
+  virtual void initField() = 0;
+  virtual void cudaSetup() = 0;
+  virtual void evolve() = 0;
+};
+
 // The full (non-APT) phase-field solver, one phi field per grain (the reference's
 // PhaseField, PhaseField.cu:431-632, selected by -a); APTPhaseField overrides
 // cudaSetup and evolve with the active-parameter-tracking solver.
-class PhaseField {
+//
+// The methods keep the reference's names, arguments and void results
+// (PhaseField.h:11-59).  The reference checks no error; here the first failure
+// is recorded (failed(), lastError()) and every later call of the sequence
+// returns without doing anything, so a caller checks once at the end.
+class PhaseField : public PDE {
  public:
-  virtual ~PhaseField();
-  // Each returns false with a message in lastError() on failure.
-  bool parseInputParams(const std::string& fileName);
-  bool cpuSetup();
-  bool initField();
-  virtual bool cudaSetup();
-  virtual bool evolve();
+  ~PhaseField() override;
+  void parseInputParams(const std::string fileName);
+  void cpuSetup(MPIsetting* mpiManager) override;
+  void initField() override;
+  void cudaSetup() override;
+  void evolve() override;
+  void OutputQoIs();
+  void OutputField(int currentStep);
   // Device candidates of the 3D junction search on the last collected argmax map
   // (cells ascending, per-cell distinct counts); false where there are none.
   virtual bool deviceJunctionCandidates(std::vector<long long>&, std::vector<unsigned char>&) {
     return false;
   }
-  bool OutputQoIs();
-  bool OutputField(int currentStep);
+  void SetMPIManager(MPIsetting* mpiManager) { mMPIManager = mpiManager; }
+  MPIsetting* GetMPIManager() const { return mMPIManager; }
   void SetDesignSetting(const DesignSettingData* d) { mDesignSetting = d; }
   const DesignSettingData* GetSetDesignSetting() const { return mDesignSetting; }
+  bool failed() const { return !mErr.empty(); }
   const std::string& lastError() const { return mErr; }
 
   int fnx = 0, fny = 0, fnz = 0, fnz_f = 0, NUM_PF = 0;
@@ -122,7 +175,7 @@ class PhaseField {
   std::vector<int> alpha, alpha_i_full;
   ThermalInputData mac;
   GlobalConstants params;
-  std::unique_ptr<QOI> qois;
+  QOI* qois = nullptr;  // set by the caller (main.cpp:58-65); owned and deleted here
   QoiGrid qoiGrid() const;
   std::string outputBaseName() const;
   cupf_apt_params deviceParams() const;
@@ -130,11 +183,19 @@ class PhaseField {
 
  protected:
   bool setErr(const std::string& e) {
-    mErr = e;
+    if (mErr.empty()) mErr = e;
     return false;
   }
   bool check(cupf_status st, const char* what);
+  bool parseInputImpl(const std::string& fileName);
+  bool cpuSetupImpl(MPIsetting* mpiManager);
+  bool initFieldImpl();
+  bool denseCudaSetup();
+  bool denseEvolve();
+  bool outputQoIsImpl();
+  bool outputFieldImpl(int currentStep);
   const DesignSettingData* mDesignSetting = nullptr;
+  MPIsetting* mMPIManager = nullptr;
   std::string mErr;
   cupf_dense_handle* mDense = nullptr;
 };
@@ -142,14 +203,16 @@ class PhaseField {
 class APTPhaseField : public PhaseField {
  public:
   ~APTPhaseField() override;
-  bool cudaSetup() override;
-  bool evolve() override;
+  void cudaSetup() override;
+  void evolve() override;
   bool deviceJunctionCandidates(std::vector<long long>& cells,
                                 std::vector<unsigned char>& distinct) override;
   cupf_apt_handle* handle() const { return mHandle; }
   cupf_precision precision = CUPF_PREC_FP32;
 
  protected:
+  bool aptCudaSetup();
+  bool aptEvolve();
   bool moveDomain(MovingDomain* md);
   bool getLineQoIs(MovingDomain* md);
   bool collectToHost(bool clear);

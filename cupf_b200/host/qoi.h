@@ -15,6 +15,8 @@
 
 namespace cupf_host {
 
+struct GlobalConstants;  // phase_field.h
+
 struct QoiGrid {
   int fnx = 0, fny = 0, fnz = 0;
   int num_theta = 0;  // NG
@@ -39,6 +41,7 @@ class QOI {
 class QOILine : public QOI {
  public:
   explicit QOILine(const QoiGrid& g);
+  explicit QOILine(const GlobalConstants& params);  // the reference's constructor
   void searchJunctionsOnImage(const QoiGrid& g, const int* alpha) override;
 
  private:
@@ -48,6 +51,7 @@ class QOILine : public QOI {
 class QOI3D : public QOI {
  public:
   explicit QOI3D(const QoiGrid& g);
+  explicit QOI3D(const GlobalConstants& params);  // the reference's constructor
   void searchJunctionsOnImage(const QoiGrid& g, const int* alpha) override;
   // The same records from the device's ascending candidate list and per-cell
   // distinct-value counts (cupf_apt_junction_candidates).

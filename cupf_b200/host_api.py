@@ -27,6 +27,8 @@ def _lib():
                                             C.c_char_p, C.c_char_p, C.c_int]
         L.cupf_host_setup.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int,
                                       _IP, _FP, _FP, _IP, C.c_int64, C.c_char_p, C.c_int]
+        L.cupf_host_setup_state.argtypes = [C.c_char_p, C.c_char_p] + [C.c_int] * 4 + [
+            _IP, _FP] + [_FP] * 6 + [_IP, _FP, _FP, C.c_int64, C.c_char_p, C.c_int]
         L.cupf_host_h5_write.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), C.c_char_p,
                                          _IP, C.POINTER(C.c_int64), C.POINTER(C.c_void_p)]
         _bound = True
@@ -104,6 +106,46 @@ def get_options(argv):
     b1, b2, b3 = (C.create_string_buffer(512) for _ in range(3))
     _lib().cupf_host_get_options(len(argv), arr, _i(out), b1, b2, b3, 511)
     return out, b1.value.decode(), b2.value.decode(), b3.value.decode()
+
+
+SETUP_FPARAMS = ("dt", "tau0", "lamd", "hi", "G", "underCoolingRate", "z0", "kin_delta", "lxd",
+                 "lyd", "lzd", "R", "V", "top", "r0", "x0", "cfl", "underCoolingRate0", "W0",
+                 "dx")
+SETUP_DIMS = ("fnx", "fny", "fnz", "num_theta", "Mt", "nts", "thermalType", "fnz_f")
+
+
+def setup_state(input_file, folder, bc=(0, 0, 0), line_config=False, pure_nucleation=False,
+                nucleation=False, cap=1 << 26):
+    """The driver's parseInputParams + cpuSetup + initField with the state the
+    reference's PhaseField holds afterwards: dict of SETUP_DIMS, SETUP_FPARAMS and
+    arrays x, y, z, z_full, phi, psi, alpha, sint, cost."""
+    dims = np.zeros(8, np.int32)
+    fp = np.zeros(20, np.float32)
+    arr = {k: np.zeros(cap, np.float32) for k in ("x", "y", "z", "z_full", "phi", "psi", "sint",
+                                                     "cost")}
+    alpha = np.zeros(cap, np.int32)
+    err = C.create_string_buffer(512)
+    flags = (1 if line_config else 0) | (2 if pure_nucleation else 0) | (4 if nucleation else 0)
+    f = lambda k: arr[k].ctypes.data_as(_FP)
+    r = _lib().cupf_host_setup_state(input_file.encode(), folder.encode(), bc[0], bc[1], bc[2],
+                                     flags, _i(dims), fp.ctypes.data_as(_FP), f("x"), f("y"),
+                                     f("z"), f("z_full"), f("phi"), f("psi"), _i(alpha), f("sint"),
+                                     f("cost"), cap, err, 511)
+    if r != 0:
+        raise RuntimeError(err.value.decode() or "capacity too small")
+    return setup_dict(dims, fp, arr, alpha)
+
+
+def setup_dict(dims, fp, arr, alpha):
+    d = dict(zip(SETUP_DIMS, (int(v) for v in dims)))
+    d.update(zip(SETUP_FPARAMS, (np.float32(v) for v in fp)))
+    L = d["fnx"] * d["fny"] * d["fnz"]
+    nt = 2 * d["num_theta"] + 1
+    for k, n in (("x", d["fnx"]), ("y", d["fny"]), ("z", d["fnz"]), ("z_full", d["fnz_f"]),
+                 ("phi", L), ("psi", L), ("sint", nt), ("cost", nt)):
+        d[k] = arr[k][:n].copy()
+    d["alpha"] = alpha[:L].copy()
+    return d
 
 
 def setup(input_file, folder, bc=(0, 0, 0), line_config=False, pure_nucleation=False,

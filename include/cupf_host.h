@@ -69,6 +69,20 @@ int cupf_host_setup(const char* input_file, const char* folder, int bcX, int bcY
                     int flags, int32_t* dims, float* fparams, float* phi, int32_t* alpha,
                     int64_t length_cap, char* err, int err_cap);
 
+/* The same set-up with the state the reference's PhaseField holds after it
+ * (PhaseFieldCpu.cpp:17-459): flags bit 2 = nucleation (includeNucleation).
+ * dims[0..7] = fnx, fny, fnz, num_theta, Mt, nts, thermalType, fnz_f;
+ * fparams[0..19] = dt, tau0, lamd, hi, G, underCoolingRate, z0, kin_delta, lxd,
+ * lyd, lzd, R, V, top, r0, x0, cfl, underCoolingRate0, W0, dx.  x / y / z /
+ * z_full receive fnx / fny / fnz / fnz_f coordinates; phi, psi, alpha (fnx*fny*fnz)
+ * and sint, cost (2*num_theta+1) are copied when cap is large enough; any
+ * output may be NULL.  Returns 0, 1 when cap was too small for the arrays, or
+ * -1 with a message in err. */
+int cupf_host_setup_state(const char* input_file, const char* folder, int bcX, int bcY, int bcZ,
+                          int flags, int32_t* dims, float* fparams, float* x, float* y, float* z,
+                          float* z_full, float* phi, float* psi, int32_t* alpha, float* sint,
+                          float* cost, int64_t cap, char* err, int err_cap);
+
 /* 2D Echebarria–Karma line model (cupf_ek2d.h).  The params type is declared
  * there; these take a pointer to it. */
 struct cupf_ek2d_params;

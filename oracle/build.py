@@ -125,8 +125,10 @@ def build_ref_gpu(num_pf, force=False):
     cpp = [os.path.join(REF_DIR, f) for f in ("helper.cpp", "QOI.cpp", "MovingDomain.cpp",
                                                  "MPIsetting.cpp", "DesignSettingData.cpp",
                                                  "ThermalInputData.cpp")]
-    cpp.append(os.path.join(HERE, "ref", "ref_host_stubs.cpp"))
-    deps = cu + cpp + [apt, __file__, os.path.join(HERE, "ref", "mpi.h")]
+    # the reference's host set-up, compiled against the stub hdf5.h of oracle/ref
+    cpp += [os.path.join(REF_DIR, "PhaseFieldCpu.cpp"), os.path.join(HERE, "ref", "ref_setup_shim.cpp")]
+    deps = cu + cpp + [apt, __file__, os.path.join(HERE, "ref", "mpi.h"),
+                       os.path.join(HERE, "ref", "hdf5.h")]
     if not force and _newer(out, deps):
         return out
     objdir = os.path.join(OUT, "obj%d" % num_pf)
@@ -163,9 +165,10 @@ def build_ref_dense(force=False):
     cpp = [os.path.join(REF_DIR, f) for f in ("helper.cpp", "QOI.cpp", "MovingDomain.cpp",
                                                  "MPIsetting.cpp", "DesignSettingData.cpp",
                                                  "ThermalInputData.cpp")]
-    cpp.append(os.path.join(HERE, "ref", "ref_host_stubs.cpp"))
+    cpp.append(os.path.join(REF_DIR, "PhaseFieldCpu.cpp"))  # against the stub hdf5.h
     deps = cu + cpp + [os.path.join(REF_DIR, "PhaseField.cu"), __file__,
-                       os.path.join(HERE, "ref", "mpi.h"), os.path.join(ROOT, "include", "cupf.h")]
+                       os.path.join(HERE, "ref", "mpi.h"), os.path.join(HERE, "ref", "hdf5.h"),
+                       os.path.join(ROOT, "include", "cupf.h")]
     if not force and _newer(out, deps):
         return out
     objdir = os.path.join(OUT, "obj_dense")

@@ -62,3 +62,53 @@ def test_setup_reads_alpha3d_field(tmp_path, monkeypatch, built):
     np.savetxt(folder / "alpha3D.txt", ids[:-1], fmt="%d")
     with pytest.raises(RuntimeError, match="alpha3D"):
         host_api.setup("line.py", str(folder), bc=(1, 1, 0))
+
+
+CASES = [
+    # input file name (sets thermalType), line configuration, pure nucleation, bc, extra files
+    ("line.py", True, False, (1, 1, 0), {}),
+    ("line.py", False, False, (0, 0, 0), {}),
+    ("line.py", True, True, (1, 0, 0), {}),
+    ("cylinder.py", False, False, (1, 1, 0), {}),
+    ("cone.py", True, False, (0, 1, 1), {"angle.txt": "0.7\n", "V.txt": "0.2\n"}),
+    ("paraboloid.py", True, False, (1, 1, 0), {"mp_len.txt": "1.6\n", "V.txt": "0.5\n"}),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "%s_line%d_pure%d_bc%d%d%d" % (
+    c[0][:-3], c[1], c[2], *c[3]))
+def test_setup_matches_reference_host_code(tmp_path, monkeypatch, built, case):
+    """The driver's parseInputParams + cpuSetup + initField against the
+    reference's own PhaseFieldCpu.cpp:17-459 (compiled unmodified, with a stub
+    hdf5.h whose reads return zeros, into oracle/_ref) on the same input file and
+    forcing folder: every derived parameter, coordinate array, the interpolated
+    psi and phi, the substrate ids and the orientation sines and cosines, bit for
+    bit."""
+    try:
+        from oracle import RefSetup
+        ref = RefSetup()
+    except (FileNotFoundError, OSError) as e:
+        pytest.skip("reference host code not built: %s" % e)
+    name, line, pure, bc, extra = case
+    Lx, Ly, Lz = 2.48, 1.92, 4.96  # the macro grid covers asp_ratio_zx = 2
+    folder = tmp_path / "forcing" / "case5"
+    preprocess.write_line_forcing(str(folder), Lx, Ly, Lz, num_grains=11, seed=5, G=2.0,
+                                  R=0.4, z0=0.55, top=0.4, t_end=1e-6)
+    for fname, text in extra.items():
+        (folder / fname).write_text(text)
+    preprocess.write_input_file(str(tmp_path / name), Lx, nts=3, asp_ratio_yx=Ly / Lx,
+                                asp_ratio_zx=2.0, moving_ratio=0.75 if line else 1.0, num_pf=6,
+                                extra={"kin_delta": 0.07})
+    monkeypatch.chdir(tmp_path)
+    kw = dict(bc=bc, line_config=line, pure_nucleation=pure, cap=1 << 20)
+    mine = host_api.setup_state(name, str(folder), **kw)
+    theirs = ref.setup(name, str(folder), **kw)
+    assert mine.keys() == theirs.keys()
+    for k, v in theirs.items():
+        if isinstance(v, np.ndarray):
+            assert v.dtype == mine[k].dtype and v.shape == mine[k].shape, k
+            assert np.array_equal(mine[k].view(np.int32), v.view(np.int32)), k
+        else:
+            assert np.array_equal(np.float32(mine[k]).view(np.int32),
+                                  np.float32(v).view(np.int32)) if isinstance(v, np.floating) \
+                else mine[k] == v, (k, mine[k], v)
