@@ -1,0 +1,6 @@
+// DesignSettingData.h — for callers written against the reference's headers
+// (3DgrainMPI/DesignSettingData.h): the driver's DesignSettingData (phase_field.h) under the reference's name.
+#pragma once
+#include "MPIsetting.h"
+#include "../phase_field.h"
+using cupf_host::DesignSettingData;

@@ -1,0 +1,6 @@
+// ThermalInputData.h — for callers written against the reference's headers
+// (3DgrainMPI/ThermalInputData.h): the driver's ThermalInputData (phase_field.h) under the reference's name.
+#pragma once
+#include "MPIsetting.h"
+#include "../phase_field.h"
+using cupf_host::ThermalInputData;

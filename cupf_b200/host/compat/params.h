@@ -1,0 +1,6 @@
+// params.h — for callers written against the reference's headers
+// (3DgrainMPI/params.h): the driver's GlobalConstants (phase_field.h) under the reference's name.
+#pragma once
+#include "MPIsetting.h"
+#include "../phase_field.h"
+using cupf_host::GlobalConstants;

@@ -141,6 +141,14 @@ static QoiGrid qoi_grid_of(const GlobalConstants& p) {
 QOILine::QOILine(const GlobalConstants& params) : QOILine(qoi_grid_of(params)) {}
 QOI3D::QOI3D(const GlobalConstants& params) : QOI3D(qoi_grid_of(params)) {}
 
+bool PhaseField::setErr(const std::string& e) {
+  if (mErr.empty()) {
+    mErr = e;
+    std::fprintf(stderr, "cupf PhaseField: %s\n", e.c_str());
+  }
+  return false;
+}
+
 bool PhaseField::check(cupf_status st, const char* what) {
   if (st == CUPF_OK) return true;
   return setErr(std::string(what) + ": " + cupf_last_error());

@@ -182,10 +182,9 @@ class PhaseField : public PDE {
   int device = 0;
 
  protected:
-  bool setErr(const std::string& e) {
-    if (mErr.empty()) mErr = e;
-    return false;
-  }
+  // records the first failure and prints it to stderr (a caller written for the
+  // reference's void methods, such as its main.cpp, checks nothing)
+  bool setErr(const std::string& e);
   bool check(cupf_status st, const char* what);
   bool parseInputImpl(const std::string& fileName);
   bool cpuSetupImpl(MPIsetting* mpiManager);

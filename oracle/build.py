@@ -8,7 +8,12 @@ Outputs
   oracle/_ref/libref_apt5.so    reference kernels (APTPhaseField.cu, PhaseField.cu,
                                 ...) compiled for sm_100a, NUM_PF=5 as shipped,
                                 with launchers (ref/ref_harness.cu)
-  oracle/_ref/libref_aptN.so    the same with APT_NUM_PF set to N (N = 1..8)
+  oracle/_ref/libref_aptN.so    the same with APT_NUM_PF set to N (N = 1..8), plus the
+                                reference's host set-up (PhaseFieldCpu.cpp against the
+                                stub ref/hdf5.h) behind ref/ref_setup_shim.cpp
+  oracle/_ref/ref_main_on_cupf  the reference's main.cpp (copied unmodified into
+                                _ref/main_on_cupf/) built against the library's
+                                headers of the reference's names and libcupf.so
   oracle/_ref/libref_dense.so   reference full-PF kernels (PhaseField.cu, unmodified)
                                 with launchers (ref/ref_dense_harness.cu)
   oracle/_ref/libref_ek2d.so    reference 2D line-model kernels and setup()
@@ -209,8 +214,35 @@ def build_ref_ek2d(force=False):
     return out
 
 
+def build_ref_main(force=False):
+    """The reference's own driver (3DgrainMPI/main.cpp, unmodified) compiled
+    against the library's headers of the reference's names
+    (cupf_b200/host/compat) and linked to cupf_b200/libcupf.so: it shows the
+    drop-in surface.  The file is copied into oracle/_ref/main_on_cupf first,
+    because its quoted includes would otherwise resolve next to it in the
+    reference tree.  Needs the library built."""
+    src = os.path.join(REF_DIR, "main.cpp")
+    lib = os.path.join(ROOT, "cupf_b200", "libcupf.so")
+    if not os.path.isfile(src) or not os.path.isfile(lib):
+        return None
+    d = os.path.join(OUT, "main_on_cupf")
+    os.makedirs(d, exist_ok=True)
+    out = os.path.join(OUT, "ref_main_on_cupf")
+    compat = os.path.join(ROOT, "cupf_b200", "host", "compat")
+    deps = [src, lib, __file__] + [os.path.join(compat, f) for f in os.listdir(compat)] + [
+        os.path.join(ROOT, "cupf_b200", "host", f) for f in ("phase_field.h", "qoi.h")]
+    if not force and _newer(out, deps):
+        return out
+    shutil.copyfile(src, os.path.join(d, "main.cpp"))
+    _run(["g++", "-O2", "-std=c++17", "-w", "-I", compat, os.path.join(d, "main.cpp"), "-o", out,
+          "-L", os.path.dirname(lib), "-lcupf", "-Wl,-rpath,$ORIGIN/../../cupf_b200",
+          "-L" + CUDA_LIB, "-lcudart", "-Wl,-rpath," + CUDA_LIB])
+    return out
+
+
 def build_all(force=False):
     outs = [build_oracle(force)]
+    outs.append(build_ref_main(force))
     outs.append(build_ref_host(force))
     outs.append(build_ref_ek2d(force))
     outs.append(build_ref_dense(force))

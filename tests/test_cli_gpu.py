@@ -97,3 +97,36 @@ def test_phase_field_cli_nucleation_from_temperature_table(tmp_path, built):
     d, _ = _nucleation_run(tmp_path, "c", 2, 0)
     g2p = d["grainToPF"]
     assert len(g2p) > 0 and np.all(g2p > 9)
+
+
+def test_reference_main_runs_on_the_library(tmp_path, built):
+    """The reference's own driver (3DgrainMPI/main.cpp, unmodified), compiled
+    against the library's headers of the reference's names and linked to
+    libcupf.so (oracle/_ref/ref_main_on_cupf, built where the reference tree
+    exists), runs the line case and writes the same file, dataset for dataset,
+    as the library's phase_field."""
+    ref_exe = os.path.join(ROOT, "oracle", "_ref", "ref_main_on_cupf")
+    if not os.path.exists(ref_exe):
+        pytest.skip("reference main not built")
+    Lx = 2.48
+    folder = tmp_path / "forcing" / "case0"
+    preprocess.write_line_forcing(str(folder), Lx, Lx, 2 * Lx, num_grains=10, seed=0, G=1.0,
+                                  R=0.05, z0=0.6, top=0.3, t_end=5e-7)
+    preprocess.write_input_file(str(tmp_path / "line.py"), Lx, nts=2, asp_ratio_zx=2.0,
+                                moving_ratio=1.0, num_pf=8)
+    outs = []
+    for exe in (os.path.join(ROOT, "cupf_b200", "phase_field"), ref_exe):
+        out = tmp_path / ("out_" + os.path.basename(exe))
+        out.mkdir()
+        r = subprocess.run([exe, "line.py", "-s", "0", "-b", "110", "-l", "1", "-o", str(out)],
+                           cwd=tmp_path, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr + r.stdout
+        assert "cupf PhaseField" not in r.stderr, r.stderr
+        files = sorted(os.listdir(out))
+        assert len(files) == 1 and files[0].endswith(".h5"), files
+        outs.append((files[0], H5File(str(out / files[0]))))
+    (na, a), (nb, b) = outs
+    assert na == nb
+    assert a.keys() == b.keys() and "tip_y" in a.keys()
+    for k in a.keys():
+        assert np.array_equal(a[k], b[k]), k
