@@ -174,7 +174,7 @@ class _Fp64Stepper:
     def step(self):
         p = self.case.params
         self.n += 1
-        t = float(np.float32(np.float32(self.n) * np.float32(p.dt)) * np.float32(p.tau0))
+        t = float(self.n) * float(p.dt) * float(p.tau0)  # FP64 time
         self.o.set_bc(p, self.ph, self.ids)
         self.o.rhs_psi_f64(self.case, t, self.ph, self.ids, self.ph_b, self.ids_b)
         self.ph, self.ph_b = self.ph_b, self.ph
@@ -488,6 +488,88 @@ def run_ek2d(args):
     return 0
 
 
+MELT_INTERIOR = (256, 256, 768)
+MELT_GRAINS = 400
+TIPP = 20  # moving-domain check interval of the reference's line runs (APTPhaseField.cu:29)
+
+
+def run_meltpool(args):
+    """Moving-domain melt-pool configuration at its stated size: a 256 x 256 x 768
+    window, 400 substrate grains, NUM_PF = 8, the analytic paraboloid pool
+    (radius 60 um, length 120 um, 0.5 m/s scan, G = 1 K/um; thermalType 5),
+    Philox nucleation at undercooling N(10 K, 2 K) from the same field's 4-D
+    table, the frame check every 20 steps, in FP32 and FP16 storage.  Per
+    storage: `steps` steps of the reference's loop order (step, nucleation pass,
+    frame check, step) timed on the host clock around synchronised work, and the
+    step kernel alone over the same state with CUDA events."""
+    import torch
+    from cupf_b200 import cases
+    from cupf_b200.solver import APTSolver
+    torch.cuda.set_device(0)
+    nx, ny, nz = MELT_INTERIOR if not args.interior else tuple(args.interior)
+    grains = max(10, int(MELT_GRAINS * nx * ny / (MELT_INTERIOR[0] * MELT_INTERIOR[1])))
+    cells = nx * ny * nz
+    steps = args.steps - (args.steps % 2)
+    warm = args.warmup + (args.warmup % 2)
+    peak, src = measured_peak()
+    res = {}
+    for prec in ("fp32", "fp16"):
+        d = cases.derive_params({**cases.LINE_CONSTANTS, "R": 0.5})
+        t_end = (warm + steps + 2 * TIPP) * float(d["dt"]) * float(d["tau0"])
+        case = cases.meltpool_case(nx, ny, nz, num_pf=NUM_PF, num_grains=grains, seed=SEED,
+                                   t_end=t_end)
+        p = case.params
+        thres = int(0.8 * p.fnz)
+        with APTSolver(case, precision=prec) as s:
+            s.set_skip_quiet(False)  # every work item computed, as the reference sweeps
+            s.init_from_argmax(case.phi, case.alpha)
+            s.nucl_init()
+            state = {"tip": 1, "mc": 0, "moved": 0, "nuclei": 0}
+
+            def pair(it):
+                s.step(1)
+                state["nuclei"] = s.nucleate(False)
+                if (2 * it + 2) % TIPP == 0:
+                    state["tip"], state["mc"], m = s.move_domain(state["tip"], thres, state["mc"])
+                    state["moved"] += m
+                s.step(1)
+
+            for it in range(warm // 2):
+                pair(it)
+            s.sync()
+            with ClockSampler(0) as clk:
+                t0 = time.perf_counter()
+                for it in range(warm // 2, (warm + steps) // 2):
+                    pair(it)
+                s.sync()
+                wall = time.perf_counter() - t0
+            kern_ms = s.time_steps(max(steps, 20)) / max(steps, 20)
+        bpc = NUM_PF * (16 if prec == "fp32" else 8)
+        res[prec] = {"mcell_upd_per_s": cells * steps / wall / 1e6, "ms_per_step": wall * 1e3 / steps,
+                     "step_kernel_ms": kern_ms,
+                     "step_kernel_mcell_upd_per_s": cells / kern_ms / 1e3,
+                     "hbm_gbs": cells * bpc / (kern_ms * 1e-3) / 1e9,
+                     "roofline_frac": cells * bpc / (kern_ms * 1e-3) / 1e9 / peak,
+                     "frame_shifts": state["moved"], "nuclei": state["nuclei"],
+                     "clocks": clk.summary()}
+    head = res["fp32"]
+    out = {"metric": "3D APT melt-pool Mcell-upd/s", "value": head["mcell_upd_per_s"],
+           "unit": "Mcell-upd/s", "n_gpus": 1, "steps": steps, "warmup": warm,
+           "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+           "config": {"workload": "melt pool %dx%dx%d window, %d grains, NUM_PF=%d, analytic "
+                                  "paraboloid r0=60 um V=0.5 m/s, Philox nucleation N(10 K, 2 K), "
+                                  "moving domain" % (nx, ny, nz, grains, NUM_PF),
+                      "loop": "step, nucleation pass, frame check every 20 steps, step (the "
+                              "reference's evolve order); every work item computed"},
+           "roofline": {"bound": "hbm", "achieved": head["hbm_gbs"], "peak": peak, "unit": "GB/s",
+                        "frac": head["roofline_frac"], "traffic": None, "peak_source": src,
+                        "of": "step kernel alone, window cells x 128 B"},
+           "precisions": res, "clocks": head["clocks"], "gpu_launches": steps}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 DENSE_INTERIOR = (128, 128, 128)
 DENSE_GRAINS = 80   # the line case's grain density of 600 grains on 256x256
 
@@ -636,7 +718,7 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp16"])
     ap.add_argument("--interior", type=int, nargs=3, metavar=("NX", "NY", "NZ"),
                     help="smaller line case for profiling (grains scale with the xy area)")
-    ap.add_argument("--workload", default="apt3d", choices=["apt3d", "ek2d", "dense"],
+    ap.add_argument("--workload", default="apt3d", choices=["apt3d", "ek2d", "dense", "meltpool"],
                     help="ek2d: the split-precision 2D dendrite benchmark; dense: the full-PF "
                          "(-a) mode against the reference kernels and the APT step")
     ap.add_argument("--ek2d-grid", type=int, nargs=2, metavar=("NX", "NY"))
@@ -656,6 +738,8 @@ def main():
         return run_ek2d(args)
     if args.workload == "dense":
         return run_dense(args)
+    if args.workload == "meltpool":
+        return run_meltpool(args)
 
     return run_apt3d(args, ws, rank, local)
 

@@ -281,3 +281,88 @@ def paraboloid_case(nx_int: int, ny_int: int, nz_int: int, num_pf: int = 5, num_
     c.psi_mac = psi.astype(F32).reshape(-1)  # x fastest (index kx + ky*Nx + kz*Nx*Ny)
     c.meta.update(kind="paraboloid", V=V, mp_len=float(p.mp_len), curvature=curvature, order=order)
     return c
+
+
+def paraboloid_dist(p, x, y, z, t):
+    """Distance field of the analytic paraboloid melt pool (thermalType 5) in
+    FP64: the beam at x_b = x0 + V 1e6 t moves in +x along the axis y = lyd/2,
+    z = z0 + lzd; at distance xi behind it the pool's radius about the axis is
+    R = r0 sqrt(1 - xi/mp_len); ahead of it the pool ends in a hemisphere of
+    radius r0; past the tail (xi >= mp_len) the distance is to the axis.
+    Positive outside the pool (solid side); T = -G dist - UC 1e6 t."""
+    xi = float(p.x0) + float(p.V) * 1e6 * t - np.asarray(x, np.float64)
+    u = np.asarray(y, np.float64) - 0.5 * float(p.lyd)
+    w = float(p.z0) + float(p.lzd) - np.asarray(z, np.float64)
+    rr = u * u + w * w
+    mp = float(p.mp_len)
+    R = float(p.r0) * np.sqrt(np.clip(1.0 - xi / mp, 0.0, None))
+    return np.where(xi <= 0, np.sqrt(rr + xi * xi) - float(p.r0),
+                    np.where(xi < mp, np.sqrt(rr) - R, np.sqrt(rr)))
+
+
+def meltpool_case(nx_int: int, ny_int: int, nz_int: int, num_pf: int = 8, num_grains: int = 400,
+                  seed: int = 0, r0: float = 60.0, V: float = 0.5, mp_len: float = 120.0,
+                  G: float = 1.0, front_frac: float = 0.75, t_end: float = 1e-4,
+                  undcool_mean: float = 10.0, undcool_std: float = 2.0, nuc_nmax: float = 0.01,
+                  bc: str = "110", **kw) -> Case:
+    """Moving-domain melt-pool configuration with the analytic paraboloid
+    undercooling (thermalType 5; the reference tabulates its pool instead,
+    thermalType 4): pool radius r0 (um) at the beam, length mp_len (um) behind it,
+    scan speed V (m/s) in +x, gradient G (K/um) normal to the pool surface, no
+    uniform cooling.  The beam starts at the window's far x edge with the pool
+    surface there at front_frac of the window height, so the front rises through
+    the window's moving threshold as the pool passes.  The initial phase field is
+    tanh(dist / (W0 sqrt2)) with the substrate's grain ids in the solid; the 4-D
+    temperature table that nucleation reads (Temp.h5's role) samples the same
+    field on a 9 x 9 x Nz x 6 grid up to t_end (the window's z range after the
+    largest shift the run can make), with nucleation at undercooling N(mean, std)
+    K and density nuc_nmax per um^3."""
+    c = line_case(nx_int, ny_int, nz_int, num_pf, num_grains, seed, G=G, R=V, bc=bc, **kw)
+    p = c.params
+    dxd = F32(F32(p.dx) * F32(p.W0))
+    lxd = F32((p.fnx - 3) * dxd)
+    p.thermalType = 5
+    p.V = F32(V)
+    p.r0 = F32(r0)
+    p.mp_len = F32(mp_len)
+    p.x0 = lxd
+    p.z0 = F32(F32(front_frac) * p.lzd + F32(r0) - p.lzd)  # axis at z0 + lzd
+    p.underCoolingRate = F32(0.0)
+    p.undcool_mean = F32(undcool_mean)
+    p.undcool_std = F32(undcool_std)
+    p.nuc_Nmax = F32(nuc_nmax)
+    p.nuc_Nmax0 = F32(nuc_nmax)
+    fnz, fny, fnx = c.shape
+    zz, yy, xx = np.meshgrid(c.z.astype(np.float64), c.y.astype(np.float64),
+                             c.x.astype(np.float64), indexing="ij")
+    dist = paraboloid_dist(p, xx, yy, zz, 0.0)
+    phi = np.zeros((fnz, fny, fnx), F32)
+    inner = np.tanh(dist / (float(p.W0) * math.sqrt(2.0))).astype(F32)
+    phi[1:-1, 1:-1, 1:-1] = inner[1:-1, 1:-1, 1:-1]
+    full = np.zeros((fny, fnx), np.int32)
+    full[1:-1, 1:-1] = c.substrate
+    solid = phi.astype(np.float64) > LS
+    alpha = np.where(solid, full[None], 0).astype(np.int32)
+    c.phi = phi.reshape(-1)
+    c.alpha = alpha.reshape(-1)
+    # 4-D temperature table for nucleation
+    Nx = Ny = 9
+    rise = float(V) * 1e6 * t_end  # the pool passes by this much: bound on the window's shift
+    zmax = float(c.z[-1]) + rise + 2 * float(dxd)
+    Nz = max(9, int(math.ceil((zmax - float(c.z[0])) / float(4 * dxd))) + 1)
+    Nt = 6
+    X = np.linspace(float(c.x[0]), float(c.x[-1]), Nx).astype(F32)
+    Y = np.linspace(float(c.y[0]), float(c.y[-1]), Ny).astype(F32)
+    Z = np.linspace(float(c.z[0]), zmax, Nz).astype(F32)
+    tm = np.linspace(0.0, t_end, Nt).astype(F32)
+    T = np.empty((Nt, Nz, Ny, Nx), np.float64)
+    zg, yg, xg = np.meshgrid(Z.astype(np.float64), Y.astype(np.float64), X.astype(np.float64),
+                             indexing="ij")
+    for it in range(Nt):
+        T[it] = -float(p.G) * paraboloid_dist(p, xg, yg, zg, float(tm[it]))
+    p.Nx, p.Ny, p.Nz, p.Nt = Nx, Ny, Nz, Nt
+    c.X_mac, c.Y_mac, c.Z_mac, c.t_mac = X, Y, Z, tm
+    c.T_3D = T.astype(F32).reshape(-1)  # x fastest, t slowest
+    c.meta.update(kind="meltpool", r0=r0, V=V, mp_len=mp_len, G=G, front_frac=front_frac,
+                  t_end=t_end)
+    return c

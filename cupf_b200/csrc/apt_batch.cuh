@@ -50,6 +50,7 @@ __global__ void __launch_bounds__(NTHREADS, step_min_blocks<NP, S>())
     a.use_iuc = sd->use_iuc;
     // t of step n (1-based) = (float)n * dt * tau0, as the single-simulation path
     a.t = __fmul_rn(__fmul_rn((float)(sd->steps + 1), a.dt), a.tau0);
+    a.t64 = __dmul_rn(__dmul_rn((double)(sd->steps + 1), (double)a.dt), (double)a.tau0);
     a.sr_key = (uint32_t)(sd->steps + 1);
     if (a.quiet_out && item_quiet(a, w.y, w.z, w.w)) continue;
     step_item<NP, S>(tmaps + 2 * w.x + cur, a, w.y, w.z, w.w, sm, qbase);

@@ -33,6 +33,12 @@ struct StepArgs {
   int ntx, nty, nzc, zc;  // tile grid and z-chunk length
   int num_theta, thermalType, use_iuc;
   float t;
+  // time and height coordinates in FP64 (fp64 != 0: 16-bit storage, whose long
+  // runs keep time, the moving-domain offset and the thermal model's
+  // coordinates in double); t and z are the reference's FP32 forms
+  int fp64;
+  double t64;
+  const double* z64;
   uint32_t sr_key;  // per-step key of the stochastic-rounding bits (16-bit storage)
   float kin_delta, eps, G, z0, uc, uc0, L_cp, hi, lamd, dt, tau0;
   float lyd, lzd, r0, x0, angle, V, mp_len, order;

@@ -138,7 +138,68 @@ __device__ __forceinline__ float interp3d(const float* __restrict__ u, float x, 
 // Undercooling at (i,j,k) and time t (APTPhaseField.cu:278-327).  Returns false
 // where the reference skips the update (`continue`: the slot keeps what the
 // output buffer already holds).
+// The thermal models with time and height in FP64 (16-bit storage): the same
+// formulas as tinterp below, every product and sum in double, the coordinates
+// x, y (fixed, exact in float) promoted and z from the FP64 copy; the
+// trilinear table lookup of thermalType 4 interpolates the float table at the
+// double coordinates rounded to float.
+__device__ __forceinline__ bool tinterp64(const StepArgs& a, int i, int j, int k, float* T) {
+  const double t = a.t64;
+  const double uct = (double)a.uc * 1e6 * t;
+  if (a.use_iuc) {
+    *T = (float)(-(double)a.uc0 * 1e6 * t);
+    return true;
+  }
+  const double z = a.z64[k];
+  if (a.thermalType == 1) {
+    *T = (float)((double)a.G * (z - (double)a.z0) - uct);
+    return true;
+  }
+  if (a.thermalType == 2) {
+    const double u = (double)__ldg(a.y + j) - 0.5 * (double)a.lyd;
+    const double v = z - (double)a.z0 - (double)a.lzd;
+    *T = (float)(-(double)a.G * (sqrt(u * u + v * v) - (double)a.r0) - uct);
+    return true;
+  }
+  if (a.thermalType == 3) {
+    const double lm = ((double)a.r0 - (double)a.z0) / tan((double)a.angle);
+    const double xl = (double)__ldg(a.x + i);
+    const double r0x = (double)a.z0 + ((double)a.r0 - (double)a.z0) * xl / lm;
+    const double u = (double)__ldg(a.y + j) - 0.5 * (double)a.lyd;
+    const double zt = (double)a.z0 + (double)a.lzd - z;
+    const double dist = cos((double)a.angle) * (sqrt(zt * zt + u * u) - r0x);
+    if (xl > (double)a.V * 1e6 * t + lm) return false;
+    *T = (float)(-(double)a.G * dist - uct);
+    return true;
+  }
+  if (a.thermalType == 5) {
+    const double xi = (double)a.x0 + (double)a.V * 1e6 * t - (double)__ldg(a.x + i);
+    const double u = (double)__ldg(a.y + j) - 0.5 * (double)a.lyd;
+    const double w = (double)a.z0 + (double)a.lzd - z;
+    const double rr = u * u + w * w;
+    double dist;
+    if (xi <= 0.0) dist = sqrt(rr + xi * xi) - (double)a.r0;
+    else if (xi < (double)a.mp_len) dist = sqrt(rr) - (double)a.r0 * sqrt(1.0 - xi / (double)a.mp_len);
+    else dist = sqrt(rr);
+    *T = (float)(-(double)a.G * dist - uct);
+    return true;
+  }
+  if (a.thermalType == 4) {
+    const double xq = (double)__ldg(a.x + i) - (double)a.V * 1e6 * t;
+    if (xq > (double)a.mp_len + (double)a.x0 || xq < 0.0) return false;
+    const float Dx = fsub(__ldg(a.X_mac + 1), __ldg(a.X_mac));
+    const float v = interp3d(a.psi_mac, (float)(xq - (double)__ldg(a.X_mac)),
+                             (float)((double)__ldg(a.y + j) - (double)__ldg(a.Y_mac)),
+                             (float)(z - (double)__ldg(a.Z_mac)), a.Nx, a.Ny, a.Nz, Dx);
+    *T = (a.order == 100.0f) ? -v : (float)(-(double)a.G * (double)v);
+    return true;
+  }
+  *T = 0.0f;
+  return true;
+}
+
 __device__ __forceinline__ bool tinterp(const StepArgs& a, int i, int j, int k, float* T) {
+  if (a.fp64) return tinterp64(a, i, j, k, T);
   const float t = a.t;
   if (a.use_iuc) {
     *T = __double2float_rn(__dmul_rn(__dmul_rn((double)(-a.uc0), 1e6), (double)t));
@@ -180,6 +241,28 @@ __device__ __forceinline__ bool tinterp(const StepArgs& a, int i, int j, int k, 
     float v = interp3d(a.psi_mac, fsub(xq, __ldg(a.X_mac)), fsub(__ldg(a.y + j), __ldg(a.Y_mac)),
                        fsub(__ldg(a.z + k), __ldg(a.Z_mac)), a.Nx, a.Ny, a.Nz, Dx);
     *T = (a.order == 100.0f) ? -v : fmul(-a.G, v);
+    return true;
+  }
+  if (a.thermalType == 5) {
+    // analytic paraboloid melt pool (no counterpart in the reference, which
+    // tabulates its pool, thermalType 4): a beam at x_b = x0 + V 1e6 t moving in
+    // +x along the axis y = lyd/2, z = z0 + lzd; behind it the pool's radius
+    // about the axis is R = r0 sqrt(1 - xi/mp_len) at distance xi, ahead of it
+    // the pool ends in a hemisphere of radius r0; dist = distance from the axis
+    // minus R (the axis itself past the tail), T = -G dist - UC 1e6 t as the cone
+    const float xb = __double2float_rn(
+        __dadd_rn((double)a.x0, __dmul_rn((double)fmul(a.V, t), 1e6)));
+    const float xi = fsub(xb, __ldg(a.x + i));
+    const float u = fsub(__ldg(a.y + j), fmul(0.5f, a.lyd));
+    const float w = fsub(fadd(a.z0, a.lzd), __ldg(a.z + k));
+    const float rr = fadd(fmul(u, u), fmul(w, w));
+    float dist;
+    if (xi <= 0.0f) dist = fsub(__fsqrt_rn(fadd(rr, fmul(xi, xi))), a.r0);
+    else if (xi < a.mp_len)
+      dist = fsub(__fsqrt_rn(rr), fmul(a.r0, __fsqrt_rn(fsub(1.0f, __fdiv_rn(xi, a.mp_len)))));
+    else dist = __fsqrt_rn(rr);
+    const double m = __dmul_rn((double)a.uc, 1e6);
+    *T = __double2float_rn(__dsub_rn((double)fmul(-a.G, dist), __dmul_rn(m, (double)t)));
     return true;
   }
   *T = 0.0f;

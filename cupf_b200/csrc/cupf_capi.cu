@@ -80,6 +80,8 @@ struct cupf_apt_handle {
   cudaStream_t stream = nullptr;
   // device inputs
   float *x = nullptr, *y = nullptr, *z = nullptr, *sint = nullptr, *cost = nullptr;
+  double* z64 = nullptr;             // z in FP64 (16-bit storage: FP64 time and heights)
+  std::vector<double> z64_host;
   float* orient = nullptr;  // packed orientation table (pack_orientations)
   float *X_mac = nullptr, *Y_mac = nullptr, *Z_mac = nullptr, *t_mac = nullptr;
   float *psi_mac = nullptr, *T_3D = nullptr;
@@ -197,7 +199,7 @@ static void free_handle(cupf_apt_handle* h) {
                   h->xfer_ph, h->xfer_id, h->layer_sums, h->alpha_full, h->loss_area,
                   h->counts, h->first, h->qoi_part, h->nucl_status, h->nucl_count,
                   h->nucl_sphere, h->jcand, h->jcount, h->jdistinct, h->quiet[0], h->quiet[1],
-                  h->active_cells};
+                  h->active_cells, h->z64};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -264,6 +266,11 @@ static StepArgs step_args(cupf_apt_handle* h, float t, int use_iuc) {
   a.thermalType = p.thermalType;
   a.use_iuc = use_iuc;
   a.t = t;
+  // 16-bit storage keeps time and heights in FP64; FP32 keeps the reference's
+  // float forms (bit parity)
+  a.fp64 = h->prec != CUPF_PREC_FP32;
+  a.t64 = (double)(h->steps_done + 1) * (double)p.dt * (double)p.tau0;
+  a.z64 = h->z64;
   a.kin_delta = p.kin_delta;
   a.eps = p.eps;
   a.G = p.G;
@@ -465,6 +472,10 @@ extern "C" cupf_status cupf_apt_create(const cupf_apt_params* p, const cupf_apt_
   TRY(upload(&h->y, in->y, p->fny, h->stream));
   TRY(upload(&h->z, in->z, p->fnz, h->stream));
   h->z_host.assign(in->z, in->z + p->fnz);
+  h->z64_host.assign(in->z, in->z + p->fnz);
+  TRY(cuda(cudaMalloc((void**)&h->z64, p->fnz * sizeof(double)), "z64"));
+  TRY(cuda(cudaMemcpyAsync(h->z64, h->z64_host.data(), p->fnz * sizeof(double),
+                           cudaMemcpyHostToDevice, h->stream), "z64 upload"));
   TRY(upload(&h->sint, in->sint, nth, h->stream));
   TRY(upload(&h->cost, in->cost, nth, h->stream));
   {
@@ -985,6 +996,13 @@ extern "C" cupf_status cupf_apt_move_domain(cupf_apt_handle* h, int32_t* tip_fro
     for (int k = 1; k < p.fnz - 2; ++k) z[k] = z[k + 1];
     z[p.fnz - 2] = ztop;
     CK(cudaMemcpyAsync(h->z, z.data(), p.fnz * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    // the same shift of the FP64 heights: the window offset accumulates in double
+    std::vector<double>& z2 = h->z64_host;
+    const double ztop2 = 2.0 * z2[p.fnz - 2] - z2[p.fnz - 3];
+    for (int k = 1; k < p.fnz - 2; ++k) z2[k] = z2[k + 1];
+    z2[p.fnz - 2] = ztop2;
+    CK(cudaMemcpyAsync(h->z64, z2.data(), p.fnz * sizeof(double), cudaMemcpyHostToDevice,
+                       h->stream));
     CK(cudaStreamSynchronize(h->stream));
     *move_count += 1;
     *tip_front -= 1;

@@ -73,6 +73,7 @@ struct Request {
   Grid g;
   void* buf[2] = {nullptr, nullptr};
   float *dx = nullptr, *dy = nullptr, *dz = nullptr, *dsint = nullptr, *dcost = nullptr;
+  double* dz64 = nullptr;  // heights in FP64 (16-bit storage)
   float* dorient = nullptr;
   float* dphi = nullptr;
   int* dalpha = nullptr;
@@ -137,12 +138,13 @@ static int gridn(long long n) {
 }
 
 static void free_request_device(Request* r) {
-  void* ptrs[] = {r->buf[0], r->buf[1], r->dx, r->dy, r->dz, r->dsint, r->dcost, r->dorient, r->dphi,
+  void* ptrs[] = {r->buf[0], r->buf[1], r->dx, r->dy, r->dz, r->dz64, r->dsint, r->dcost, r->dorient, r->dphi,
                   r->dalpha, r->ddummy, r->dquiet[0], r->dquiet[1]};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   r->buf[0] = r->buf[1] = nullptr;
   r->dx = r->dy = r->dz = r->dsint = r->dcost = r->dorient = r->dphi = nullptr;
+  r->dz64 = nullptr;
   r->dalpha = nullptr;
   r->ddummy = nullptr;
   r->dquiet[0] = r->dquiet[1] = nullptr;
@@ -234,6 +236,11 @@ static cupf_status admit(cupf_server* s, Request* r, int slot) {
       (e = up(&r->dorient, r->orient)) || (e = up(&r->dphi, r->phi)))
     return e;
   (void)nth;
+  {
+    std::vector<double> z64(r->z.begin(), r->z.end());
+    CK(cudaMalloc((void**)&r->dz64, z64.size() * sizeof(double)));
+    CK(cudaMemcpy(r->dz64, z64.data(), z64.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
   CK(cudaMalloc((void**)&r->dalpha, L * sizeof(int)));
   CK(cudaMemcpyAsync(r->dalpha, r->alpha.data(), L * sizeof(int), cudaMemcpyHostToDevice, st));
   CK(cudaMalloc((void**)&r->ddummy, 64 * sizeof(float)));
@@ -320,6 +327,8 @@ static cupf_status admit(cupf_server* s, Request* r, int slot) {
   a.x = r->dx;
   a.y = r->dy;
   a.z = r->dz;
+  a.z64 = r->dz64;
+  a.fp64 = s->cfg.precision != CUPF_PREC_FP32;
   a.sint = r->dsint;
   a.cost = r->dcost;
   a.orient = reinterpret_cast<const float4*>(r->dorient);

@@ -239,6 +239,31 @@ static int tinterp_f32(const cupf_apt_params* p, const cupf_apt_inputs* th, int 
     float v = interp3d_f32(th->psi_mac, xq - th->X_mac[0], th->y[j] - th->Y_mac[0],
                            th->z[k] - th->Z_mac[0], p->Nx, p->Ny, p->Nz, Dx);
     T = (p->order == 100.0f) ? -v : -p->G * v;
+  } else if (p->thermalType == 5) {
+    /* the library's analytic paraboloid melt pool (apt_update.cuh tinterp, no
+       counterpart in the reference), every operation rounded separately */
+    float vt = p->V * t;
+    float xb = (float)((double)p->x0 + (double)vt * 1e6);
+    float xi = xb - th->x[i];
+    float u = th->y[j] - 0.5f * p->lyd;
+    float w = (p->z0 + p->lzd) - th->z[k];
+    float uu = u * u, ww = w * w;
+    float rr = uu + ww;
+    float dist;
+    if (xi <= 0.0f) {
+      float xx = xi * xi;
+      dist = sqrtf(rr + xx) - p->r0;
+    } else if (xi < p->mp_len) {
+      float q = xi / p->mp_len;
+      float R = p->r0 * sqrtf(1.0f - q);
+      dist = sqrtf(rr) - R;
+    } else {
+      dist = sqrtf(rr);
+    }
+    double m = (double)p->underCoolingRate * 1e6;
+    float gd = -p->G * dist;
+    double mt = m * (double)t;
+    T = (float)((double)gd - mt);
   }
   *Tout = T;
   return 1;
@@ -347,7 +372,7 @@ static double kine_ani_f64(double ux, double uy, double uz, double cosa, double 
 int oracle_rhs_psi_f64(const cupf_apt_params* p, const oracle_thermal_f64* th, double t,
                        const double* ph, double* ph_new, const int32_t* aarg, int32_t* aarg_new,
                        int use_iuc, int64_t* stats) {
-  if (!use_iuc && p->thermalType != 0 && p->thermalType != 1) return -1;
+  if (!use_iuc && p->thermalType != 0 && p->thermalType != 1 && p->thermalType != 5) return -1;
   grid_t g = mkgrid(p);
   const int np = g.np;
   int64_t ovf_u = 0;
@@ -366,6 +391,18 @@ int oracle_rhs_psi_f64(const cupf_apt_params* p, const oracle_thermal_f64* th, d
         if (use_iuc) T = -(double)p->underCoolingRate0 * 1e6 * t;
         else if (p->thermalType == 1)
           T = (double)p->G * (th->z[k] - (double)p->z0) - (double)p->underCoolingRate * 1e6 * t;
+        else if (p->thermalType == 5) {
+          /* analytic paraboloid melt pool in double (apt_update.cuh tinterp64) */
+          double xi = (double)p->x0 + (double)p->V * 1e6 * t - th->x[i];
+          double u = th->y[j] - 0.5 * (double)p->lyd;
+          double w = (double)p->z0 + (double)p->lzd - th->z[k];
+          double rr = u * u + w * w, dist;
+          if (xi <= 0.0) dist = sqrt(rr + xi * xi) - (double)p->r0;
+          else if (xi < (double)p->mp_len)
+            dist = sqrt(rr) - (double)p->r0 * sqrt(1.0 - xi / (double)p->mp_len);
+          else dist = sqrt(rr);
+          T = -(double)p->G * dist - (double)p->underCoolingRate * 1e6 * t;
+        }
         double Up = T / (double)p->L_cp;
         for (int a = 0; a < np; ++a) {
           int64_t o = C + (int64_t)a * g.len;
