@@ -421,8 +421,8 @@ extern "C" cupf_status cupf_apt_create(const cupf_apt_params* p, const cupf_apt_
     return fail(CUPF_ERR_UNSUPPORTED, "num_pf=%d not built (1..8)", p->num_pf);
   if (p->num_theta < 1) return fail(CUPF_ERR_INVALID, "num_theta must be >= 1");
   if (p->haloWidth != 1) return fail(CUPF_ERR_INVALID, "haloWidth must be 1");
-  if (p->thermalType < 0 || p->thermalType > 4)
-    return fail(CUPF_ERR_INVALID, "thermalType %d not in 0..4", p->thermalType);
+  if (p->thermalType < 0 || p->thermalType > 5)
+    return fail(CUPF_ERR_INVALID, "thermalType %d not in 0..5", p->thermalType);
   if (precision != CUPF_PREC_FP32 && precision != CUPF_PREC_BF16 && precision != CUPF_PREC_FP16)
     return fail(CUPF_ERR_UNSUPPORTED, "precision %d not built", (int)precision);
   if (precision != CUPF_PREC_FP32 && p->num_theta > 32767)

@@ -60,7 +60,12 @@ typedef struct cupf_apt_params {
   int32_t num_pf;         /* NUM_PF, active slots per cell (1..CUPF_MAX_PF) */
   int32_t num_theta;      /* NG: grain orientations in sint/cost */
   int32_t bcX, bcY, bcZ;  /* 0 = no-flux (mirror about 1 / fn-2), 1 = periodic */
-  int32_t thermalType;    /* 0 none, 1 line, 2 cylinder, 3 cone, 4 paraboloid table */
+  int32_t thermalType;    /* 0 none, 1 line, 2 cylinder, 3 cone, 4 paraboloid table,
+                             5 analytic paraboloid melt pool (no counterpart in the
+                             reference: a beam at x0 + V 1e6 t moving in +x along
+                             y = lyd/2, z = z0 + lzd; pool radius r0 sqrt(1 - xi/mp_len)
+                             at xi behind it, a hemisphere of radius r0 ahead;
+                             T = -G dist - UC 1e6 t) */
   int32_t Nx, Ny, Nz, Nt; /* macro thermal grid (thermalType 4, nucleation) */
   float kin_delta;        /* kinetic anisotropy strength */
   float eps;              /* |grad phi|^2 threshold in kine_ani */
