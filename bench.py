@@ -249,6 +249,11 @@ def qoi_errors(volumes, qoi, ref_volumes, ref_qoi):
             "interface_area_rel_err": float(abs(qoi[1] - ref_qoi[1]) / ref_qoi[1])}
 
 
+def within_tol(e):
+    return bool(e["volume_fraction_l1_rel_err"] <= ERROR_TOL and
+                e["interface_height_rel_err"] <= ERROR_TOL)
+
+
 def storage_errors(fix, precisions=("fp32", "fp16", "bf16")):
     """Each storage on the 64^3 line case (20 grains, NUM_PF = 5, 1000 steps,
     from init_from_argmax like every production path) against the FP64 oracle's
@@ -271,8 +276,10 @@ def storage_errors(fix, precisions=("fp32", "fp16", "bf16")):
         if "c1_f32_volumes" in fix:
             e["fp32_oracle"] = qoi_errors(fix["c1_f32_volumes"], fix["c1_f32_qoi"],
                                           fix["c1_volumes"], fix["c1_qoi"])
-        e["within_tolerance"] = bool(e["volume_fraction_l1_rel_err"] <= ERROR_TOL and
-                                     e["interface_height_rel_err"] <= ERROR_TOL)
+        if "c1_p64_volumes" in fix:
+            e["fp64_perturbed"] = qoi_errors(fix["c1_p64_volumes"], fix["c1_p64_qoi"],
+                                             fix["c1_volumes"], fix["c1_qoi"])
+        e["within_tolerance"] = within_tol(e)
         out[prec] = e
     return out
 
@@ -327,6 +334,12 @@ def serve_stream(prec, nreq, fix=None, device=0):
                     e["fp32_oracle"] = qoi_errors(fix["srv%d_f32_volumes" % i],
                                                   fix["srv%d_f32_qoi" % i],
                                                   fix["srv%d_volumes" % i], fix["srv%d_qoi" % i])
+                if "srv%d_p64_volumes" % i in fix:
+                    # how far the request's own dynamics carry one float ulp of
+                    # noise on the initial state, all in FP64
+                    e["fp64_perturbed"] = qoi_errors(fix["srv%d_p64_volumes" % i],
+                                                     fix["srv%d_p64_qoi" % i],
+                                                     fix["srv%d_volumes" % i], fix["srv%d_qoi" % i])
                 errors.append(e)
         for r in ids:
             srv.release(r)
@@ -345,9 +358,13 @@ def serve_stream(prec, nreq, fix=None, device=0):
     if errors:
         for key in ("volume_fraction_l1_rel_err", "interface_height_rel_err"):
             worst[key] = max(e[key] for e in errors)
-        worst["within_tolerance"] = bool(all(
-            e["volume_fraction_l1_rel_err"] <= ERROR_TOL and e["interface_height_rel_err"] <= ERROR_TOL
-            for e in errors))
+        worst["within_tolerance"] = bool(all(within_tol(e) for e in errors))
+        worst["results_within_tolerance"] = sum(within_tol(e) for e in errors)
+        # requests whose FP64 run from a one-ulp-perturbed start already differs
+        # from the FP64 run by more than the tolerance (the bound is below what
+        # the request's dynamics resolve)
+        worst["results_fp64_perturbed_beyond_tolerance"] = sum(
+            1 for e in errors if "fp64_perturbed" in e and not within_tol(e["fp64_perturbed"]))
     return {"precision": prec, "sims_per_hr": len(res) / span * 3600.0,
             "p50_s": float(np.percentile(ttr, 50)), "p99_s": float(np.percentile(ttr, 99)),
             "mcell_upd_per_s": cells / span / 1e6, "requests": len(res),
@@ -438,6 +455,29 @@ def run_ek2d(args):
         r["tip_err_cells"] = abs(q["tip_y"] - ref["tip_y"]) / dxd
         r["spacing_rel_err"] = (abs(q["spacing"] - ref["spacing"]) / ref["spacing"]
                                 if ref["spacing"] else None)
+    # how far the front's own dynamics carry a rounding-sized perturbation: FP64
+    # again from the initial state with psi moved by one float ulp, up or down at
+    # random, on a seeded half of the cells
+    rng = np.random.default_rng(7)
+    psi0 = np.ascontiguousarray(case.psi, np.float32)
+    move = rng.random(psi0.shape) < 0.5
+    up = rng.random(psi0.shape) < 0.5
+    psi_p = psi0.copy()
+    psi_p[move & up] = np.nextafter(psi0[move & up], np.float32(np.inf))
+    psi_p[move & ~up] = np.nextafter(psi0[move & ~up], np.float32(-np.inf))
+    with ek2d.EK2DSolver(case, precision="fp64") as sv:
+        sv.set_state(psi_p, case.U)
+        sv.prestep()
+        sv.step(steps)
+        st = sv.get_state()
+        y = sv.get_y()
+    q = ek2d.qois(st["phi"], y, dxd)
+    res["fp64_perturbed"] = {
+        "what": "FP64 from the initial psi with one float ulp of noise on half the cells",
+        "qois": q, "tip_err_cells": abs(q["tip_y"] - ref["tip_y"]) / dxd,
+        "tip_advance_rel_err": abs(q["tip_y"] - ref["tip_y"]) / abs(adv) if adv else None,
+        "spacing_rel_err": (abs(q["spacing"] - ref["spacing"]) / ref["spacing"]
+                            if ref["spacing"] else None)}
     # end to end through the C ABI with host buffers: create, H2D of psi/U, the
     # pre-step and all steps, D2H of the final fields
     t0 = time.perf_counter()

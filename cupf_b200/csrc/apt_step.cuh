@@ -482,7 +482,9 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
       }
       const float nv = slot_update(a, kc, ph7, sina, cosa, sinb, cosb, repul, Up);
       const int oid = (nv < kDrop) ? -1 : id;  // (double)nv < -0.9999
-      if (S::kStochastic) return S::make_sr(nv, oid, mix32(cell_key + (uint32_t)j * 0x9E3779B9u));
+      // slot j's rounding bits: the cell's hashed key times a distinct odd
+      // constant per slot (a bijection of a uniform 32-bit value, one multiply)
+      if (S::kStochastic) return S::make_sr(nv, oid, cell_key * ((uint32_t)(2 * j + 1) * 0x9E3779B9u));
       return S::make(nv, oid);
     };
     if (RolledSlots<S>::value) {

@@ -1,9 +1,9 @@
 // apt_storage.cuh — storage formats of one (phi, grain id) slot pair.
 //
 // PairF32: the reference's own precision, {float phi, int32 id} in 8 bytes.
-// PairH16<F>: split precision, {16-bit phi, int16 id} in 4 bytes, phi in BF16
-//   or FP16 (the step stores with stochastic rounding, set-up paths round to
-//   nearest even); ids must fit in int16 (-1 = empty).
+// PairH16<F>: split precision, {16-bit phi code, int16 id} in 4 bytes, the code
+//   in BF16 or FP16 (the step stores with stochastic rounding, set-up paths
+//   round to nearest even); ids must fit in int16 (-1 = empty).
 // The step computes in FP32 for every format; only the stored pair differs.
 #pragma once
 
@@ -40,14 +40,19 @@ struct PairF32 {
 
 enum class Half16 { BF16, FP16 };
 
-// 16-bit phi is stored as its distance to the nearest bulk value,
-//   u = copysign(1, phi) - phi,   phi = copysign(1, u) - u,
-// with u = +0 for phi = +1 and u = -0 for phi = -1 (empty slots stay exact).
-// A 16-bit float keeps ~11 (FP16) or 8 (BF16) significant bits of u, i.e.
-// relative precision of 1 - |phi| where the tanh profile's tails approach the
-// bulk values and change by less than a plain 16-bit spacing per step (plain
-// FP16 spacing is 4.9e-4 for |phi| in [0.5, 1): tails stall there).  Values
-// outside [-1, 1] (rounding overshoot) are stored as +-1.
+// 16-bit phi is stored in one of two bands, told apart by the code's magnitude:
+//   |phi| >= 1/2: c = copysign(1 - |phi|, phi), |c| <= 1/2 (the distance to the
+//                 nearest bulk value: c = +0 for phi = +1, -0 for phi = -1, so
+//                 empty slots stay exact);
+//   |phi| <  1/2: c = copysign(1 + K |phi|, phi), K = 4096, |c| in [1, 2049).
+// A 16-bit float keeps ~11 (FP16) or 8 (BF16) significant bits of c: relative
+// precision of 1 - |phi| in the tanh profile's tails, which approach the bulk
+// values and change by less than a plain 16-bit spacing per step, and relative
+// precision of |phi| in the interface core, where two grains' phi cross and the
+// argmax that gives grain volumes is decided.  The coarsest spacing is 2.4e-4
+// (FP16) at |phi| near 1/2; near phi = 0 it is far finer (a distance code alone
+// spaces phi = 0 by 4.9e-4).  Values outside [-1, 1] (rounding overshoot) are
+// stored as +-1.  Both bands' decodes are exact in FP32.
 template <Half16 F>
 struct PairH16 {
   using T = uint32_t;
@@ -55,27 +60,34 @@ struct PairH16 {
   static constexpr int kBW = 36;  // 36*4 = 144 B (16 B multiple)
   static constexpr CUtensorMapDataType kTmaType = CU_TENSOR_MAP_DATA_TYPE_UINT32;
   static constexpr int kPitchAlign = 4;
+  static constexpr float kCore = 4096.0f;
   __device__ static float decode(unsigned short b) {
-    const float u = (F == Half16::BF16) ? __bfloat162float(__ushort_as_bfloat16(b))
+    const float c = (F == Half16::BF16) ? __bfloat162float(__ushort_as_bfloat16(b))
                                         : __half2float(__ushort_as_half(b));
-    return __fsub_rn(copysignf(1.0f, u), u);
+    const float s = copysignf(1.0f, c);
+    return fabsf(c) >= 1.0f ? __fmul_rn(__fsub_rn(c, s), 1.0f / kCore) : __fsub_rn(s, c);
+  }
+  // the FP32 value of the code before rounding to 16 bits
+  __device__ static float code(float ph) {
+    const float a = fabsf(ph);
+    // 1 - a is exact for a >= 1/2; clamped at 0 for overshoot past the bulk value
+    const float m = a >= 0.5f ? fmaxf(__fsub_rn(1.0f, a), 0.0f) : __fmaf_rn(a, kCore, 1.0f);
+    return copysignf(m, ph);
   }
   __device__ static unsigned short encode(float ph) {
-    // |u| = 1 - |phi| (exact for |phi| >= 0.5), clamped at 0, with phi's sign:
-    // phi = -1 gives -0, phi = +1 gives +0
-    const float u = copysignf(fmaxf(__fsub_rn(1.0f, fabsf(ph)), 0.0f), ph);
-    if (F == Half16::BF16) return __bfloat16_as_ushort(__float2bfloat16_rn(u));
-    return __half_as_ushort(__float2half_rn(u));
+    const float c = code(ph);
+    if (F == Half16::BF16) return __bfloat16_as_ushort(__float2bfloat16_rn(c));
+    return __half_as_ushort(__float2half_rn(c));
   }
-  // Stochastic rounding of the step's output (r: 32 random bits): |u| goes to
-  // the 16-bit value below or above it with probabilities proportional to its
+  // Stochastic rounding of the step's output (r: 32 random bits): the code goes
+  // to the 16-bit value below or above it with probabilities proportional to its
   // distance from the other one, so the expected stored value equals the FP32
   // result.  Round-to-nearest drops every per-step change smaller than half a
   // 16-bit spacing, which biases slowly moving interfaces; this does not.
   __device__ static unsigned short encode_sr(float ph, uint32_t r) {
-    const float u = copysignf(fmaxf(__fsub_rn(1.0f, fabsf(ph)), 0.0f), ph);
-    if (F == Half16::BF16) return sr_bf16_bits(u, r);
-    return sr_fp16_bits(u, r);
+    const float c = code(ph);
+    if (F == Half16::BF16) return sr_bf16_bits(c, r);
+    return sr_fp16_bits(c, r);
   }
   static constexpr bool kStochastic = true;
   __device__ static T make_sr(float ph, int id, uint32_t r) {
@@ -86,7 +98,7 @@ struct PairH16 {
   __device__ static T make(float ph, int id) {
     return (uint32_t)encode(ph) | ((uint32_t)(unsigned short)(short)id << 16);
   }
-  __device__ static T empty() { return 0xFFFF8000u; }  // u = -0 (phi = -1), id -1
+  __device__ static T empty() { return 0xFFFF8000u; }  // c = -0 (phi = -1), id -1
   __device__ static bool is_empty(T p) { return p == 0xFFFF8000u; }
 };
 

@@ -43,7 +43,10 @@ __device__ __forceinline__ unsigned short sr_fp16_bits(float x, uint32_t r) {
   uint32_t e = __float_as_uint(a) & 0x7F800000u;
   const uint32_t emin = (uint32_t)(127 - 14) << 23;
   e = (e < emin ? emin : e) - (10u << 23);
-  const float t = __fmaf_rn((float)(r >> 8) * 0x1p-24f, __uint_as_float(e), a);
+  // a uniform fraction in [0, 1) from the top 23 bits of r: the float 1.f
+  // with those bits as its mantissa, minus 1 (exact)
+  const float f = __fsub_rn(__uint_as_float(0x3F800000u | (r >> 9)), 1.0f);
+  const float t = __fmaf_rn(f, __uint_as_float(e), a);
   return (unsigned short)(__half_as_ushort(__float2half_rz(t)) | (sign >> 16));
 }
 
