@@ -308,6 +308,46 @@ static __global__ void junction_candidates_kernel(const int* __restrict__ alpha,
   }
 }
 
+// Candidate cells of the line-configuration junction search
+// (QOILine::searchJunctionsOnImage, QOI.cpp:103-160) over `nl` stacked x-y
+// layers of an argmax map (the layers at the sampled tip heights): interior
+// cells whose 3x3 in-plane neighbourhood holds at least three distinct values,
+// none more than five times.  out receives the cells' indices in the stacked
+// layers (layer * fnx * fny + j * fnx + i) in no particular order, up to cap;
+// count receives their number.
+static __global__ void line_junction_kernel(const int* __restrict__ layers, int nl, int fnx,
+                                            int fny, long long* out, long long cap,
+                                            unsigned long long* count) {
+  const long long ni = fnx - 2, nj = fny - 2;
+  const long long total = ni * nj * nl, plane = (long long)fnx * fny;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long i = 1 + idx % ni, j = 1 + (idx / ni) % nj, l = idx / (ni * nj);
+    const long long C = l * plane + j * fnx + i;
+    int v[9];
+#pragma unroll
+    for (int dj = -1; dj <= 1; ++dj)
+#pragma unroll
+      for (int di = -1; di <= 1; ++di) v[(dj + 1) * 3 + di + 1] = __ldg(layers + C + dj * fnx + di);
+    int nd = 0, maxc = 0;
+#pragma unroll
+    for (int a = 0; a < 9; ++a) {
+      bool first = true;
+      int c = 0;
+#pragma unroll
+      for (int b = 0; b < 9; ++b) {
+        c += (v[b] == v[a]);
+        if (b < a && v[b] == v[a]) first = false;
+      }
+      nd += first;
+      maxc = max(maxc, c);
+    }
+    if (nd < 3 || maxc > 5) continue;
+    const unsigned long long slot = atomicAdd(count, 1ull);
+    if ((long long)slot < cap) out[slot] = C;
+  }
+}
+
 // FP64 interface QoIs over the interior, from m = max-over-slots phi of each cell:
 //   part[2*b]   = sum (1 + m) / 2              (solid volume, cell units)
 //   part[2*b+1] = sum |grad m| / 2             (interface area, cell units; a

@@ -769,6 +769,51 @@ extern "C" cupf_status cupf_apt_junction_candidates(cupf_apt_handle* h, int64_t*
   return CUPF_OK;
 }
 
+extern "C" cupf_status cupf_line_junction_candidates(int32_t device, int32_t fnx, int32_t fny,
+                                                    const int32_t* layers, int32_t nlayers,
+                                                    int64_t* cells, int64_t cap, int64_t* count) {
+  if (!count || fnx < 3 || fny < 3 || nlayers < 0 || cap < 0 || (cap > 0 && !cells) ||
+      (nlayers > 0 && !layers))
+    return fail(CUPF_ERR_INVALID, "bad argument");
+  *count = 0;
+  if (nlayers == 0) return CUPF_OK;
+  CK(cudaSetDevice(device));
+  const cudaStream_t st = cudaStreamPerThread;
+  const long long plane = (long long)fnx * fny;
+  const long long ncell = (long long)(fnx - 2) * (fny - 2) * nlayers;
+  const size_t lbytes = (size_t)plane * nlayers * sizeof(int32_t);
+  const long long want = cap > 0 ? cap : 1;
+  int32_t* d_layers = nullptr;
+  long long* d_out = nullptr;
+  unsigned long long* d_count = nullptr;
+  cudaError_t e = cudaMallocAsync((void**)&d_layers, lbytes, st);
+  if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_out, want * sizeof(long long), st);
+  if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_count, sizeof(unsigned long long), st);
+  unsigned long long n = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_layers, layers, lbytes, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), st);
+  if (e == cudaSuccess) {
+    line_junction_kernel<<<grid_for(ncell), 256, 0, st>>>(d_layers, nlayers, fnx, fny, d_out, cap,
+                                                          d_count);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&n, d_count, sizeof(n), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  const long long got = std::min<long long>((long long)n, cap);
+  if (e == cudaSuccess && got > 0) {
+    e = cudaMemcpyAsync(cells, d_out, got * sizeof(long long), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  }
+  if (d_layers) cudaFreeAsync(d_layers, st);
+  if (d_out) cudaFreeAsync(d_out, st);
+  if (d_count) cudaFreeAsync(d_count, st);
+  CK(e);
+  CK(cudaStreamSynchronize(st));
+  if (got > 0) std::sort(cells, cells + got);
+  *count = (int64_t)n;
+  return CUPF_OK;
+}
+
 extern "C" cupf_status cupf_apt_grain_volumes(cupf_apt_handle* h, int32_t num_grains,
                                               int64_t* counts) {
   if (!h || !counts || num_grains < 0) return fail(CUPF_ERR_INVALID, "bad argument");

@@ -1,6 +1,7 @@
 // host_capi.cpp — C entry points of include/cupf_host.h.
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/cupf_host.h"
 #include "host_util.h"
@@ -84,6 +85,54 @@ extern "C" int cupf_host_junctions_3d_cells(int fnx, int fny, int fnz, const int
   const int n = (int)v.size();
   for (int i = 0; i < n && i < cap; ++i) nodes[i] = v[i];
   return n;
+}
+
+// QOILine::searchJunctionsOnImage (or its candidate-cell form when cells is not
+// NULL) on a full map whose frame kt has its tip layer at tip_y[kt].
+static int line_junctions(int fnx, int fny, int nts, int num_nodes, const int32_t* tip_y,
+                          const int32_t* alpha, const int64_t* cells, int64_t ncells,
+                          int32_t* nodes, int cap, int32_t* cross, int64_t cross_cap) {
+  if (fnx < 3 || fny < 3 || nts < 0 || num_nodes < 0 || !tip_y || !alpha) return -1;
+  QoiGrid g;
+  g.fnx = fnx;
+  g.fny = fny;
+  g.nts = nts;
+  g.num_nodes = num_nodes;
+  g.num_theta = 1;
+  QOILine q(g);
+  q.mQoIVectorIntData["tip_y"].assign(tip_y, tip_y + nts + 1);
+  if (cells) {
+    std::vector<long long> c(cells, cells + ncells);
+    q.searchJunctionsOnCells(g, alpha, c.data(), ncells);
+  } else {
+    q.searchJunctionsOnImage(g, alpha);
+  }
+  const std::vector<int>& v = q.mQoIVectorIntData["node_region"];
+  const int n = (int)v.size();
+  for (int i = 0; i < n && i < cap; ++i) nodes[i] = v[i];
+  const std::vector<int>& cs = q.mQoIVectorIntData["cross_sec"];
+  if (cross)
+    for (int64_t i = 0; i < (int64_t)cs.size() && i < cross_cap; ++i) cross[i] = cs[i];
+  return n;
+}
+
+extern "C" int cupf_host_line_junctions(int fnx, int fny, int nts, int num_nodes,
+                                        const int32_t* tip_y, const int32_t* alpha,
+                                        int32_t* nodes, int cap, int32_t* cross,
+                                        int64_t cross_cap) {
+  return line_junctions(fnx, fny, nts, num_nodes, tip_y, alpha, nullptr, 0, nodes, cap, cross,
+                        cross_cap);
+}
+
+extern "C" int cupf_host_line_junctions_cells(int fnx, int fny, int nts, int num_nodes,
+                                              const int32_t* tip_y, const int32_t* alpha,
+                                              const int64_t* cells, int64_t ncells,
+                                              int32_t* nodes, int cap, int32_t* cross,
+                                              int64_t cross_cap) {
+  if (ncells < 0 || (ncells > 0 && !cells)) return -1;
+  static const int64_t none = 0;
+  return line_junctions(fnx, fny, nts, num_nodes, tip_y, alpha, cells ? cells : &none, ncells,
+                        nodes, cap, cross, cross_cap);
 }
 
 extern "C" int cupf_host_h5_write(const char* path, int n, const char* const* names,

@@ -456,6 +456,37 @@ std::string PhaseField::outputBaseName() const {
          to_stringp(p.min_angle, 3) + "_order" + std::to_string((int)p.order) + grainType;
 }
 
+// The line-configuration junction search with its neighbourhood test on the
+// device: the frames' tip layers of the full map go to
+// cupf_line_junction_candidates, and the records are built for the candidate
+// cells only (the same records, in the same order, as the full host scan).
+bool PhaseField::lineJunctions(QOILine* q, const QoiGrid& g, const int* a) {
+  const int nf = g.nts + 1;
+  const long long plane = (long long)fnx * fny;
+  const std::vector<int>& tip_y = q->mQoIVectorIntData["tip_y"];
+  if ((int)tip_y.size() < nf) return setErr("line QoIs: fewer tip heights than frames");
+  std::vector<int> layers((size_t)plane * nf);
+  for (int kt = 0; kt < nf; ++kt) {
+    if (tip_y[kt] < 0 || (long long)(tip_y[kt] + 1) * plane > full_length)
+      return setErr("line QoIs: tip height outside the full map");
+    std::memcpy(layers.data() + (size_t)plane * kt, a + (size_t)plane * tip_y[kt],
+                sizeof(int) * (size_t)plane);
+  }
+  std::vector<long long> cells;
+  int64_t cap = 1 << 16, count = 0;
+  for (;;) {
+    cells.assign((size_t)cap, 0);
+    if (!check(cupf_line_junction_candidates(device, fnx, fny, layers.data(), nf,
+                                             reinterpret_cast<int64_t*>(cells.data()), cap, &count),
+               "cupf_line_junction_candidates"))
+      return false;
+    if (count <= cap) break;
+    cap = count;
+  }
+  q->searchJunctionsOnCells(g, a, cells.data(), (long long)count);
+  return true;
+}
+
 // PhaseField::OutputQoIs (PhaseFieldCpu.cpp:464-520): junction search, then the
 // coordinates, geometry scalars and every QoI vector, one 1-D dataset each.
 bool PhaseField::outputQoIsImpl() {
@@ -465,7 +496,10 @@ bool PhaseField::outputQoIsImpl() {
   std::vector<long long> cells;
   std::vector<unsigned char> distinct;
   QOI3D* q3 = dynamic_cast<QOI3D*>(qois);
-  if (ds->useLineConfig)
+  QOILine* ql = dynamic_cast<QOILine*>(qois);
+  if (ds->useLineConfig && ql) {
+    if (!lineJunctions(ql, g, alpha_i_full.data())) return false;
+  } else if (ds->useLineConfig)
     qois->searchJunctionsOnImage(g, alpha_i_full.data());
   else if (q3 && deviceJunctionCandidates(cells, distinct))
     q3->searchJunctionsOnCells(g, alpha.data(), cells.data(), (long long)cells.size(),

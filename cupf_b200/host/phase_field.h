@@ -192,6 +192,7 @@ class PhaseField : public PDE {
   bool denseCudaSetup();
   bool denseEvolve();
   bool outputQoIsImpl();
+  bool lineJunctions(QOILine* q, const QoiGrid& g, const int* a);
   bool outputFieldImpl(int currentStep);
   const DesignSettingData* mDesignSetting = nullptr;
   MPIsetting* mMPIManager = nullptr;

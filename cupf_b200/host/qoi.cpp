@@ -66,49 +66,88 @@ void QOI::calculateLineQoIs(const QoiGrid& g, int& cur_tip, const int* alpha, in
   for (int j = 0; j < ng; ++j) total[(size_t)kt * ng + j] += loss_area[j];
 }
 
+// The junction record of one cell of a line-configuration cross section, or
+// false when its 3x3 in-plane neighbourhood holds fewer than three distinct
+// values or one more than five times (the body of the reference's scan,
+// QOI.cpp:118-156; a fresh hash map per cell, as there, so the grain ids come
+// out in the same order).
+bool QOILine::lineRecord(const int* layer, int fnx, int j, int i, int* rec) const {
+  std::unordered_map<int, int> occur;
+  for (int dj = -1; dj <= 1; ++dj)
+    for (int di = -1; di <= 1; ++di) {
+      const int v = layer[(long long)(j + dj) * fnx + i + di];
+      auto it = occur.find(v);
+      if (it != occur.end())
+        it->second++;
+      else
+        occur.insert({v, 1});
+    }
+  int n_alpha = 0, max_occ = 0;
+  for (auto& it : occur) {
+    n_alpha++;
+    max_occ = std::max(max_occ, it.second);
+  }
+  if (n_alpha < 3 || max_occ > 5) return false;
+  std::fill(rec, rec + mNumNodeFeatures, -1);
+  rec[0] = i;
+  rec[1] = j;
+  rec[2] = max_occ;
+  int c = 0;
+  for (auto& it : occur)
+    if (3 + c < mNumNodeFeatures) rec[3 + c++] = it.first;
+  return true;
+}
+
+// Stores one record in frame kt's part of node_region (records past the
+// frame's preallocated capacity are dropped; the reference writes past it).
+// Features the record does not set keep the array's -1.
+void QOILine::storeRecord(int kt, int nframes, size_t& node_cnt, const int* rec) {
+  std::vector<int>& node = mQoIVectorIntData["node_region"];
+  const size_t cap = node.size() / nframes;
+  const size_t base = cap * kt;
+  if ((node_cnt + 1) * mNumNodeFeatures > cap) return;
+  for (int f = 0; f < mNumNodeFeatures; ++f)
+    if (rec[f] != -1 || f < 3) node[base + node_cnt * mNumNodeFeatures + f] = rec[f];
+  node_cnt++;
+}
+
 // QOILine::searchJunctionsOnImage (QOI.cpp:103-160): per saved tip layer, the
 // cross section and the 3x3 in-plane neighbourhoods with >= 3 grains.
 void QOILine::searchJunctionsOnImage(const QoiGrid& g, const int* alpha) {
   const int fnx = g.fnx, fny = g.fny;
-  std::vector<int>& node = mQoIVectorIntData["node_region"];
   std::vector<int>& cross = mQoIVectorIntData["cross_sec"];
   const std::vector<int>& tip_y = mQoIVectorIntData["tip_y"];
+  int rec[8];
   for (int kt = 0; kt < g.nts + 1; ++kt) {
-    const int cur_tip = tip_y[kt];
-    const long long off = (long long)fnx * fny * cur_tip;
+    const long long off = (long long)fnx * fny * tip_y[kt];
     cross.insert(cross.end(), alpha + off, alpha + off + (long long)fnx * fny);
-    const size_t base = node.size() / (g.nts + 1) * kt;
-    const size_t cap = node.size() / (g.nts + 1);
     size_t node_cnt = 0;
     for (int j = 1; j < fny - 1; ++j)
-      for (int i = 1; i < fnx - 1; ++i) {
-        std::unordered_map<int, int> occur;
-        for (int dj = -1; dj <= 1; ++dj)
-          for (int di = -1; di <= 1; ++di) {
-            const int v = alpha[off + (long long)(j + dj) * fnx + i + di];
-            auto it = occur.find(v);
-            if (it != occur.end())
-              it->second++;
-            else
-              occur.insert({v, 1});
-          }
-        int n_alpha = 0, max_occ = 0;
-        for (auto& it : occur) {
-          n_alpha++;
-          max_occ = std::max(max_occ, it.second);
-        }
-        if (n_alpha >= 3 && max_occ <= 5) {
-          if ((node_cnt + 1) * mNumNodeFeatures > cap) continue;
-          const size_t o = base + node_cnt * mNumNodeFeatures;
-          node[o] = i;
-          node[o + 1] = j;
-          node[o + 2] = max_occ;
-          int c = 0;
-          for (auto& it : occur)
-            if (3 + c < mNumNodeFeatures) node[o + 3 + c++] = it.first;
-          node_cnt++;
-        }
-      }
+      for (int i = 1; i < fnx - 1; ++i)
+        if (lineRecord(alpha + off, fnx, j, i, rec)) storeRecord(kt, g.nts + 1, node_cnt, rec);
+  }
+}
+
+// The same records from the device's candidate list: `cells` ascending, each
+// an index into the frames' tip layers stacked in frame order
+// (kt * fnx * fny + j * fnx + i), as cupf_apt_line_junction_candidates returns
+// them.
+void QOILine::searchJunctionsOnCells(const QoiGrid& g, const int* alpha, const long long* cells,
+                                     long long ncells) {
+  const int fnx = g.fnx, fny = g.fny;
+  const long long plane = (long long)fnx * fny;
+  std::vector<int>& cross = mQoIVectorIntData["cross_sec"];
+  const std::vector<int>& tip_y = mQoIVectorIntData["tip_y"];
+  int rec[8];
+  long long n = 0;
+  for (int kt = 0; kt < g.nts + 1; ++kt) {
+    const long long off = plane * tip_y[kt];
+    cross.insert(cross.end(), alpha + off, alpha + off + plane);
+    size_t node_cnt = 0;
+    for (; n < ncells && cells[n] / plane == kt; ++n) {
+      const int j = (int)((cells[n] % plane) / fnx), i = (int)(cells[n] % fnx);
+      if (lineRecord(alpha + off, fnx, j, i, rec)) storeRecord(kt, g.nts + 1, node_cnt, rec);
+    }
   }
 }
 

@@ -43,8 +43,14 @@ class QOILine : public QOI {
   explicit QOILine(const QoiGrid& g);
   explicit QOILine(const GlobalConstants& params);  // the reference's constructor
   void searchJunctionsOnImage(const QoiGrid& g, const int* alpha) override;
+  // The same records from the device's ascending candidate list over the
+  // frames' stacked tip layers (cupf_apt_line_junction_candidates).
+  void searchJunctionsOnCells(const QoiGrid& g, const int* alpha, const long long* cells,
+                              long long ncells);
 
  private:
+  bool lineRecord(const int* layer, int fnx, int j, int i, int* rec) const;
+  void storeRecord(int kt, int nframes, size_t& node_cnt, const int* rec);
   int mNumNodeFeatures = 8;
 };
 

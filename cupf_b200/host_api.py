@@ -90,6 +90,46 @@ def junctions_3d(fnx, fny, fnz, alpha, cap=1 << 22):
     return out[:n].copy()
 
 
+def line_junctions(fnx, fny, nts, num_nodes, tip_y, alpha, cells=None):
+    """QOILine::searchJunctionsOnImage on a full map (frame kt's tip layer at
+    tip_y[kt]): (node_region, cross_sec).  With `cells` (ascending candidate
+    indices into the stacked tip layers, as cupf_line_junction_candidates gives
+    them) the records are built for those cells only."""
+    cap = (nts + 1) * 5 * num_nodes * 8
+    out = np.zeros(max(cap, 1), np.int32)
+    cross = np.zeros((nts + 1) * fnx * fny, np.int32)
+    tip = np.ascontiguousarray(tip_y, np.int32)
+    a = np.ascontiguousarray(alpha, np.int32)
+    if cells is None:
+        n = _lib().cupf_host_line_junctions(fnx, fny, nts, num_nodes, _i(tip), _i(a), _i(out),
+                                            cap, _i(cross), C.c_int64(len(cross)))
+    else:
+        c = np.ascontiguousarray(cells, np.int64)
+        n = _lib().cupf_host_line_junctions_cells(
+            fnx, fny, nts, num_nodes, _i(tip), _i(a), c.ctypes.data_as(C.POINTER(C.c_int64)),
+            C.c_int64(len(c)), _i(out), cap, _i(cross), C.c_int64(len(cross)))
+    if n < 0:
+        raise ValueError("bad argument")
+    return out[:n].copy(), cross
+
+
+def line_junction_candidates(fnx, fny, layers, device=0):
+    """Device candidates of the line junction search over stacked tip layers
+    (nlayers x fny x fnx int32): ascending indices into the stack."""
+    layers = np.ascontiguousarray(layers, np.int32)
+    nl = layers.size // (fnx * fny)
+    cap = 1 << 12
+    while True:
+        cells = np.zeros(cap, np.int64)
+        count = C.c_int64()
+        abi.check(_lib().cupf_line_junction_candidates(
+            device, fnx, fny, _i(layers), nl, cells.ctypes.data_as(C.POINTER(C.c_int64)),
+            C.c_int64(cap), C.byref(count)))
+        if count.value <= cap:
+            return cells[:count.value].copy()
+        cap = count.value
+
+
 def get_param(line, key, kind=float, init=0):
     if kind is float:
         v = C.c_float(init)

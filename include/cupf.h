@@ -224,6 +224,23 @@ cupf_status cupf_apt_nucl_reset(cupf_apt_handle* h);
 cupf_status cupf_apt_junction_candidates(cupf_apt_handle* h, int64_t* cells, int64_t cap,
                                          int64_t* count, uint8_t* distinct);
 
+/* Candidate cells of the line-configuration junction search
+ * (QOILine::searchJunctionsOnImage, QOI.cpp:103-160), on device `device`.
+ * `layers` (host memory) holds `nlayers` x-y layers of fnx*fny int32 argmax
+ * values each (reference layout), one per sampled frame: the layer at that
+ * frame's tip height.  Candidates are interior cells whose 3x3 in-plane
+ * neighbourhood holds at least three distinct values and none more than five
+ * times.  Writes up to `cap` of their indices in the stacked layers
+ * (layer*fnx*fny + j*fnx + i), in ascending order, and their number to *count
+ * (which can exceed cap: call again with more room).  Building the records of
+ * the candidate cells only (cupf_host_line_junctions_cells) gives the records
+ * of the full host scan.  Needs no handle (the APT and the full-PF drivers both
+ * call it); allocates its scratch for the call, on the calling thread's
+ * per-thread stream, and returns when the result is on the host. */
+cupf_status cupf_line_junction_candidates(int32_t device, int32_t fnx, int32_t fny,
+                                          const int32_t* layers, int32_t nlayers, int64_t* cells,
+                                          int64_t cap, int64_t* count);
+
 /* Allocation-free per-grain voxel counts (no counterpart in the reference).
  * For callers that cannot let a library allocate device memory: codes that give
  * all device memory to their own pool allocator at start-up, and services whose

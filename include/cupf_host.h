@@ -39,6 +39,22 @@ int cupf_host_junctions_3d_cells(int fnx, int fny, int fnz, const int32_t* alpha
                                  const int64_t* cells, int64_t ncells, const uint8_t* distinct,
                                  int32_t* nodes, int cap);
 
+/* QOILine::searchJunctionsOnImage (QOI.cpp:103-160) on a full line-configuration
+ * map alpha (fnx*fny per layer) whose frame kt (0..nts) has its tip layer at
+ * tip_y[kt], with num_nodes the input's NN: writes up to cap ints of node
+ * records ((nts+1) frames x 5*NN records x 8 ints: i, j, max_occur, up to 5
+ * grain ids, -1 padding) and, when cross is not NULL, up to cross_cap ints of
+ * the frames' cross sections; returns the record length used, or -1. */
+int cupf_host_line_junctions(int fnx, int fny, int nts, int num_nodes, const int32_t* tip_y,
+                             const int32_t* alpha, int32_t* nodes, int cap, int32_t* cross,
+                             int64_t cross_cap);
+
+/* The same records from the device's candidates: `cells` (ascending) as
+ * cupf_line_junction_candidates returns them for the frames' tip layers. */
+int cupf_host_line_junctions_cells(int fnx, int fny, int nts, int num_nodes, const int32_t* tip_y,
+                                   const int32_t* alpha, const int64_t* cells, int64_t ncells,
+                                   int32_t* nodes, int cap, int32_t* cross, int64_t cross_cap);
+
 /* h5write_1d of a whole file (3DgrainMPI/PhaseFieldCpu.cpp:584-613, as OutputQoIs /
  * OutputField use it): writes n 1-D datasets into the root group of a new HDF5
  * file at path (superblock version 0, contiguous little-endian data).  Dataset

@@ -65,6 +65,25 @@ int refq_junctions_3d(int fnx, int fny, int fnz, const int* alpha, int* nodes, i
   return n;
 }
 
+// QOILine::searchJunctionsOnImage (QOI.cpp:103-160) on a full map whose frame
+// kt has its tip layer at tip_y[kt].  Writes node_region (up to cap) and the
+// cross sections (up to cross_cap); returns node_region's length.
+int refq_line_junctions(int fnx, int fny, int nts, int num_nodes, const int* tip_y,
+                        const int* alpha, int* nodes, int cap, int* cross, long long cross_cap) {
+  GlobalConstants p;
+  std::memset(&p, 0, sizeof(p));
+  p.fnx = fnx; p.fny = fny; p.nts = nts; p.num_nodes = num_nodes; p.num_theta = 1;
+  QOILine q(p);
+  for (int kt = 0; kt <= nts; ++kt) q.mQoIVectorIntData["tip_y"][kt] = tip_y[kt];
+  q.searchJunctionsOnImage(p, alpha);
+  const std::vector<int>& v = q.mQoIVectorIntData["node_region"];
+  const int n = (int)v.size();
+  for (int i = 0; i < n && i < cap; ++i) nodes[i] = v[i];
+  const std::vector<int>& c = q.mQoIVectorIntData["cross_sec"];
+  for (long long i = 0; i < (long long)c.size() && i < cross_cap; ++i) cross[i] = c[i];
+  return n;
+}
+
 // QOI::sampleHeights (QOI.cpp:162-185).
 int refq_sample_heights(int* cur_tip, const int* alpha, int fnx, int fny, int fnz) {
   GlobalConstants p;

@@ -119,3 +119,78 @@ def test_device_candidates_equal_full_scan(built, precision):
     assert np.array_equal(cells, want_cells)
     assert np.array_equal(distinct, want_distinct)
     assert np.array_equal(host_cells(a, cells, distinct), host_full(a))
+
+
+# ---- line configuration (QOILine::searchJunctionsOnImage, QOI.cpp:103-160) ----
+
+def line_map(fnx, fny, fnz, grains, seed):
+    """A full line-configuration map: columnar 2D Voronoi grains (ids 1..grains,
+    halo included) whose layout changes with height, liquid (0) in the top
+    planes."""
+    rng = np.random.default_rng(seed)
+    a = np.zeros((fnz, fny, fnx), np.int32)
+    y, x = np.meshgrid(np.arange(fny), np.arange(fnx), indexing="ij")
+    pts = rng.random((grains, 2)) * (fny, fnx)
+    for k in range(fnz - 3):
+        pts += rng.normal(0, 0.4, pts.shape)  # grains drift with height
+        d = (y[..., None] - pts[:, 0]) ** 2 + (x[..., None] - pts[:, 1]) ** 2
+        a[k] = np.argmin(d, axis=-1) + 1
+    return np.ascontiguousarray(a)
+
+
+def numpy_line_candidates(a, tip_y):
+    """Candidates over the stacked tip layers, computed without the library."""
+    fnz, fny, fnx = a.shape
+    cells = []
+    for kt, t in enumerate(tip_y):
+        L = a[t]
+        nb = np.stack([L[1 + dj:fny - 1 + dj, 1 + di:fnx - 1 + di]
+                       for dj in (-1, 0, 1) for di in (-1, 0, 1)])
+        s = np.sort(nb, axis=0)
+        distinct = np.concatenate([np.ones((1,) + s.shape[1:], bool), s[1:] != s[:-1]]).sum(0)
+        run = np.ones(s.shape, np.int32)
+        for q in range(1, 9):
+            run[q] = np.where(s[q] == s[q - 1], run[q - 1] + 1, 1)
+        cand = (distinct >= 3) & (run.max(axis=0) <= 5)
+        jj, ii = np.nonzero(cand)
+        cells.append(kt * fny * fnx + (jj + 1) * fnx + (ii + 1))
+        assert distinct[cand].max(initial=0) <= 5  # the reference writes past a record beyond 5 ids
+    return np.concatenate(cells).astype(np.int64)
+
+
+LINE_CASES = [  # fnx, fny, fnz, grains, seed, tip_y
+    (34, 30, 24, 25, 0, [3, 7, 7, 12, 20]),
+    (20, 41, 16, 12, 4, [1, 5, 9]),
+    (50, 12, 10, 30, 9, [2, 6]),
+]
+
+
+@pytest.mark.parametrize("spec", LINE_CASES, ids=lambda s: "%dx%dx%d" % s[:3])
+def test_line_junctions_match_reference_and_candidates(built, spec):
+    from cupf_b200 import host_api
+    from oracle import RefHost
+    fnx, fny, fnz, grains, seed, tip_y = spec
+    a = line_map(fnx, fny, fnz, grains, seed)
+    nts, nn = len(tip_y) - 1, 40
+    full, cross = host_api.line_junctions(fnx, fny, nts, nn, tip_y, a.reshape(-1))
+    rnodes, rcross = RefHost().line_junctions(fnx, fny, nts, nn, tip_y, a.reshape(-1))
+    assert np.array_equal(full, rnodes) and np.array_equal(cross, rcross)
+    cells = numpy_line_candidates(a, tip_y)
+    assert len(cells) > 0
+    got, gcross = host_api.line_junctions(fnx, fny, nts, nn, tip_y, a.reshape(-1), cells=cells)
+    assert np.array_equal(got, full) and np.array_equal(gcross, cross)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("spec", LINE_CASES, ids=lambda s: "%dx%dx%d" % s[:3])
+def test_line_junction_device_candidates(built, spec):
+    from cupf_b200 import host_api
+    fnx, fny, fnz, grains, seed, tip_y = spec
+    a = line_map(fnx, fny, fnz, grains, seed)
+    layers = np.stack([a[t] for t in tip_y])
+    cells = host_api.line_junction_candidates(fnx, fny, layers)
+    assert np.array_equal(cells, numpy_line_candidates(a, tip_y))
+    nts = len(tip_y) - 1
+    got, _ = host_api.line_junctions(fnx, fny, nts, 40, tip_y, a.reshape(-1), cells=cells)
+    full, _ = host_api.line_junctions(fnx, fny, nts, 40, tip_y, a.reshape(-1))
+    assert np.array_equal(got, full)
