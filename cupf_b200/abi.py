@@ -125,6 +125,15 @@ def lib():
             "cupf_host_junctions_3d_cells": [C.c_int] * 3 + [C.POINTER(C.c_int32),
                                              C.POINTER(C.c_int64), C.c_int64,
                                              C.POINTER(C.c_uint8), C.POINTER(C.c_int32), C.c_int],
+            "cupf_line_junction_candidates": [C.c_int32, C.c_int32, C.c_int32,
+                                              C.POINTER(C.c_int32), C.c_int32,
+                                              C.POINTER(C.c_int64), C.c_int64,
+                                              C.POINTER(C.c_int64)],
+            "cupf_host_line_junctions": [C.c_int] * 4 + [C.POINTER(C.c_int32)] * 3 + [
+                C.c_int, C.POINTER(C.c_int32), C.c_int64],
+            "cupf_host_line_junctions_cells": [C.c_int] * 4 + [C.POINTER(C.c_int32)] * 2 + [
+                C.POINTER(C.c_int64), C.c_int64, C.POINTER(C.c_int32), C.c_int,
+                C.POINTER(C.c_int32), C.c_int64],
             "cupf_grain_volumes_noalloc": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                            C.POINTER(C.c_int64), vp],
             "cupf_dense_create": [C.POINTER(cupf_apt_params), C.POINTER(cupf_apt_inputs), C.c_float,
