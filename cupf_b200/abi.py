@@ -134,6 +134,10 @@ def lib():
             "cupf_host_line_junctions_cells": [C.c_int] * 4 + [C.POINTER(C.c_int32)] * 2 + [
                 C.POINTER(C.c_int64), C.c_int64, C.POINTER(C.c_int32), C.c_int,
                 C.POINTER(C.c_int32), C.c_int64],
+            "cupf_host_voronoi_substrate": [C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int,
+                                            C.POINTER(C.c_int32), FP],
+            "cupf_host_write_substrate": [C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_int32),
+                                          C.c_int, FP],
             "cupf_grain_volumes_noalloc": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                            C.POINTER(C.c_int64), vp],
             "cupf_dense_create": [C.POINTER(cupf_apt_params), C.POINTER(cupf_apt_inputs), C.c_float,

@@ -23,7 +23,7 @@ CU_SOURCES = [os.path.join(HERE, "csrc", f)
                         "cupf_dense.cu")]
 CPP_SOURCES = [os.path.join(HERE, "host", f) for f in
                ("host_util.cpp", "qoi.cpp", "phase_field.cpp", "npz_writer.cpp", "h5_writer.cpp",
-                "host_capi.cpp", "ek2d_host.cpp")]
+                "host_capi.cpp", "ek2d_host.cpp", "substrate.cpp")]
 MAIN = os.path.join(HERE, "host", "main.cpp")
 MAIN2D = os.path.join(HERE, "host", "ek2d_main.cpp")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -39,15 +39,35 @@ def write_input_file(path, Lx, nts=2, asp_ratio_yx=1.0, asp_ratio_zx=2.0, moving
         f.write("\n".join(lines) + "\n")
 
 
+def native_substrate(nxp, nyp, num_grains, seed, periodic=True):
+    """(alpha (nyp, nxp) int32, theta (2*num_grains+1,) float32) from the
+    library's seeded Voronoi generator (cupf_host_voronoi_substrate)."""
+    from . import abi
+    import ctypes as C
+    alpha = np.zeros((nyp, nxp), np.int32)
+    theta = np.zeros(2 * num_grains + 1, np.float32)
+    r = abi.lib().cupf_host_voronoi_substrate(nxp, nyp, num_grains, C.c_uint64(seed),
+                                              1 if periodic else 0,
+                                              alpha.ctypes.data_as(C.POINTER(C.c_int32)),
+                                              theta.ctypes.data_as(C.POINTER(C.c_float)))
+    if r != 0:
+        raise ValueError("bad substrate arguments")
+    return alpha, theta
+
+
 def write_line_forcing(folder, Lx, Ly, Lz, num_grains, seed, G, R, z0, top, t_end,
                        periodic=True, macro=(13, 13, 23, 11), dxd=0.08, nmax=0.01,
-                       cooling_rate=None):
+                       cooling_rate=None, substrate="cases"):
     """The forcing folder of a line run: macro grid, psi = z0 - z, substrate ids
     (alpha.txt, (nx+1)x(ny+1) values), orientations, scalars.  nmax is the
     nucleation density (Nmax.txt).  With cooling_rate (K/s) the folder also holds
     the 4-D temperature table Temp.txt (the reference's Temp.h5:/Temp, x fastest,
     t slowest) of a uniform melt cooling from the melting point,
-    T - Tmelt = -cooling_rate * t, which nucleation reads."""
+    T - Tmelt = -cooling_rate * t, which nucleation reads.
+
+    substrate: "cases" (the numpy generator the in-memory test cases use),
+    "native" (the library's C++ generator), or an (alpha, theta) pair made
+    elsewhere, e.g. by the reference's own graph() (alpha (ny+1, nx+1))."""
     os.makedirs(folder, exist_ok=True)
     nxm, nym, nzm, ntm = macro
     BC = Lx / (nxm - 3)
@@ -59,8 +79,16 @@ def write_line_forcing(folder, Lx, Ly, Lz, num_grains, seed, G, R, z0, top, t_en
     psi = (z0 - zz).reshape(-1, order="F")
     nx = int(round(Lx / dxd))
     ny = int(round(Ly / dxd))
-    alpha = voronoi_substrate(nx + 1, ny + 1, num_grains, seed, periodic)
-    theta = grain_angles(num_grains, seed)
+    if isinstance(substrate, str) and substrate == "native":
+        alpha, theta = native_substrate(nx + 1, ny + 1, num_grains, seed, periodic)
+    elif isinstance(substrate, str):
+        alpha = voronoi_substrate(nx + 1, ny + 1, num_grains, seed, periodic)
+        theta = grain_angles(num_grains, seed)
+    else:
+        alpha, theta = (np.asarray(a) for a in substrate)
+        if alpha.shape != (ny + 1, nx + 1) or len(theta) != 2 * num_grains + 1:
+            raise ValueError("substrate shape %s / %d angles do not fit a %dx%d map of %d grains"
+                             % (alpha.shape, len(theta), nx + 1, ny + 1, num_grains))
     uc = G * R * 1e6 * 1e-6  # K/us
 
     def put(name, arr, fmt="%1.4e"):

@@ -55,6 +55,25 @@ int cupf_host_line_junctions_cells(int fnx, int fny, int nts, int num_nodes, con
                                    const int32_t* alpha, const int64_t* cells, int64_t ncells,
                                    int32_t* nodes, int cap, int32_t* cross, int64_t cross_cap);
 
+/* Seeded 2D Voronoi substrate of nxp x nyp macro pixels (a line run's alpha.txt
+ * holds (nx+1) x (ny+1) of them) with num_grains grains, for forcing folders
+ * made without the reference's Python generator (graph_datastruct.py:194-271,
+ * whose output format it keeps).  alpha (nxp*nyp, rows of constant y) gets each
+ * pixel's grain id 1..num_grains: the nearest of num_grains seeded points, with
+ * minimum-image distances when periodic is nonzero.  theta (2*num_grains+1)
+ * gets [0, theta_x[1..NG], theta_z[1..NG]] from a Gaussian random vector per
+ * grain (theta_x = atan2(u_y,u_x) mod pi, theta_z = atan2(|u_xy|,u_z) mod pi, as
+ * graph_datastruct.py:256-269).  Same seed, same output.  Returns 0, or -1 on a
+ * bad argument. */
+int cupf_host_voronoi_substrate(int nxp, int nyp, int num_grains, uint64_t seed, int periodic,
+                                int32_t* alpha, float* theta);
+
+/* Writes alpha.txt ("%d" per line), theta.txt ("%1.4e" per line) and NG.txt
+ * into an existing folder, as the reference's input scripts save them
+ * (input_file.py:148-152).  Returns 0, or -1 on a bad argument or write. */
+int cupf_host_write_substrate(const char* folder, int nxp, int nyp, const int32_t* alpha,
+                              int num_grains, const float* theta);
+
 /* h5write_1d of a whole file (3DgrainMPI/PhaseFieldCpu.cpp:584-613, as OutputQoIs /
  * OutputField use it): writes n 1-D datasets into the root group of a new HDF5
  * file at path (superblock version 0, contiguous little-endian data).  Dataset
