@@ -255,9 +255,9 @@ cupf_status cupf_line_junction_candidates(int32_t device, int32_t fnx, int32_t f
  * exits.  num_grains above CUPF_NOALLOC_MAX_GRAINS is rejected
  * (CUPF_ERR_INVALID).  Work is queued on `stream` (a cudaStream_t, NULL for
  * the default stream) on the current device, and the call returns after the
- * counts are in host memory.  The first call on a device looks up the scratch
- * address (cudaGetSymbolAddress); make that first call before any stream
- * capture.  Every call shares the one scratch array and clears it first, so
+ * counts are in host memory (the call is synchronous).  The first call on a
+ * device looks up the scratch address (cudaGetSymbolAddress).  Every call
+ * shares the one scratch array and clears it first, so
  * calls whose GPU work overlaps (different streams or threads on one device)
  * race and must be serialised by the caller. */
 #define CUPF_NOALLOC_MAX_GRAINS 65535
