@@ -79,19 +79,19 @@ struct PairH16 {
     if (F == Half16::BF16) return __bfloat16_as_ushort(__float2bfloat16_rn(c));
     return __half_as_ushort(__float2half_rn(c));
   }
-  // Stochastic rounding of the step's output (r: 32 random bits): the code goes
-  // to the 16-bit value below or above it with probabilities proportional to its
-  // distance from the other one, so the expected stored value equals the FP32
-  // result.  Round-to-nearest drops every per-step change smaller than half a
-  // 16-bit spacing, which biases slowly moving interfaces; this does not.
-  __device__ static unsigned short encode_sr(float ph, uint32_t r) {
-    const float c = code(ph);
-    if (F == Half16::BF16) return sr_bf16_bits(c, r);
-    return sr_fp16_bits(c, r);
-  }
   static constexpr bool kStochastic = true;
+  // The step's store, with stochastic rounding (r: 32 random bits, of which the
+  // hardware conversion cvt.rs uses r[31:16]): the code goes to the 16-bit
+  // value below or above it with probabilities proportional to its distance
+  // from the other one, so the expected stored value equals the FP32 result.
+  // Round-to-nearest drops every per-step change smaller than half a 16-bit
+  // spacing, which biases slowly moving interfaces; this does not.  The rounded
+  // code lands in the upper half of the conversion's result and is moved to the
+  // low half of the pair, beside the id.
   __device__ static T make_sr(float ph, int id, uint32_t r) {
-    return (uint32_t)encode_sr(ph, r) | ((uint32_t)(unsigned short)(short)id << 16);
+    const float c = code(ph);
+    const uint32_t d = (F == Half16::BF16) ? sr_pack_bf16x2(c, 0.0f, r) : sr_pack_fp16x2(c, 0.0f, r);
+    return __byte_perm(d, (uint32_t)id, 0x5432);
   }
   __device__ static float phi(T p) { return decode((unsigned short)(p & 0xFFFFu)); }
   __device__ static int id(T p) { return (int)(short)(p >> 16); }

@@ -70,6 +70,10 @@ struct StPlain {
   }
   __device__ static V st_ps(T ps) { return ps; }
   __device__ static V st_ps_sr(T ps, uint32_t) { return ps; }
+  __device__ static void st_ps_U_sr(T ps, T u, uint32_t, V& vps, V& vu) {
+    vps = ps;
+    vu = u;
+  }
 };
 using StF32 = StPlain<float>;
 using StF64 = StPlain<double>;
@@ -107,7 +111,11 @@ struct StH16 {
     return BF ? __bfloat16_as_ushort(__float2bfloat16_rn(x)) : __half_as_ushort(__float2half_rn(x));
   }
   __device__ static V stU(T x, T U0) { return st(__fsub_rn(x, U0)); }
-  __device__ static V st_sr(T x, uint32_t r) { return BF ? sr_bf16_bits(x, r) : sr_fp16_bits(x, r); }
+  // stochastic rounding by the hardware conversion (cvt.rs): x with r[31:16]
+  __device__ static uint32_t sr2(T hi, T lo, uint32_t r) {
+    return BF ? sr_pack_bf16x2(hi, lo, r) : sr_pack_fp16x2(hi, lo, r);
+  }
+  __device__ static V st_sr(T x, uint32_t r) { return (V)(sr2(x, 0.0f, r) >> 16); }
   __device__ static void ld_pp(V v, T inv_sqrt2, T& ps, T& ph) {
     if (!BF) {
       ps = ld(v);
@@ -129,6 +137,13 @@ struct StH16 {
   }
   __device__ static V st_ps(T ps) { return st(code(ps)); }
   __device__ static V st_ps_sr(T ps, uint32_t r) { return st_sr(code(ps), r); }
+  // the phase field's code and U - U0 in one conversion: r[31:16] round the
+  // first, r[15:0] the second
+  __device__ static void st_ps_U_sr(T ps, T u, uint32_t r, V& vps, V& vu) {
+    const uint32_t d = sr2(code(ps), u, r);
+    vps = (V)(d >> 16);
+    vu = (V)(d & 0xFFFFu);
+  }
 };
 using StF16 = StH16<false>;
 using StBF16 = StH16<true>;
@@ -320,12 +335,16 @@ __device__ __forceinline__ void cell_update(const EkArgs& a, const Consts<T>& c,
   const T psn = psC + c.dt * dps + noise;
   V vps, vU, vD;
   if (S::kSR) {
-    // one 32-bit draw per cell and step: independent 10-bit fractions for the
-    // phase field and U (1/1024 of a 16-bit spacing is ample); dpsi is
-    // rewritten from scratch every step, not accumulated, so it rounds to nearest
+    // one 32-bit draw per cell and step: its two 16-bit halves round the
+    // phase field and U independently; dpsi is rewritten from scratch every
+    // step, not accumulated, so it rounds to nearest
     const uint32_t r = mix32((uint32_t)(gi + a.fnx * gj) ^ step_key);
-    vps = S::st_ps_sr(psn, r & 0xFFC00000u);
-    vU = merge ? S::st_sr(Un - c.U0, (r << 10) & 0xFFC00000u) : S::stU(Un, c.U0);
+    if (merge) {
+      S::st_ps_U_sr(psn, Un - c.U0, r, vps, vU);
+    } else {
+      vps = S::st_ps_sr(psn, r);
+      vU = S::stU(Un, c.U0);
+    }
     vD = S::st(dps);
   } else {
     vps = S::st_ps(psn);

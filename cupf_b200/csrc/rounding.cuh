@@ -4,8 +4,9 @@
 // to its distance from the other one, so the expected stored value equals the
 // FP32 value.  Round-to-nearest drops every per-step change smaller than half a
 // 16-bit spacing, which biases slowly varying fields of an explicit time step;
-// stochastic rounding does not.  The random bits come from mix32 of a counter
-// (cell, field, step), so results are reproducible.
+// stochastic rounding does not.  The rounding itself is sm_100a's conversion
+// with random bits (cvt.rs); the bits come from mix32 of a counter (cell,
+// step), so results are reproducible.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -25,29 +26,22 @@ __host__ __device__ __forceinline__ uint32_t mix32(uint32_t x) {
   return x;
 }
 
-// BF16 keeps the top 16 bits of the FP32 pattern: add 16 random bits below
-// them, then truncate the magnitude.  |x| must be below the largest finite
-// BF16 value.
-__device__ __forceinline__ unsigned short sr_bf16_bits(float x, uint32_t r) {
-  const uint32_t sign = __float_as_uint(x) & 0x80000000u;
-  const uint32_t b = (__float_as_uint(fabsf(x)) + (r >> 16)) & 0xFFFF0000u;
-  return (unsigned short)((b | sign) >> 16);
+// Stochastic rounding of two FP32 values to a packed pair of 16-bit floats in
+// one sm_100a instruction (cvt.rs): the upper half of the result is hi rounded
+// with the random bits r[31:16], the lower half lo rounded with r[15:0]; each
+// rounds down or up in magnitude with probabilities proportional to its
+// distance from the other neighbour (all-zero bits truncate toward zero),
+// subnormal results included.  |hi|, |lo| must be at most the largest finite
+// value of the format.
+__device__ __forceinline__ uint32_t sr_pack_fp16x2(float hi, float lo, uint32_t r) {
+  uint32_t d;
+  asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(r));
+  return d;
 }
-
-// FP16: the spacing at |x| is 2^(E-10) for E >= -14 (normal values) and 2^-24
-// below; add a uniform fraction of it, then round toward zero.  |x| must be at
-// most 65504.
-__device__ __forceinline__ unsigned short sr_fp16_bits(float x, uint32_t r) {
-  const uint32_t sign = __float_as_uint(x) & 0x80000000u;
-  const float a = fabsf(x);
-  uint32_t e = __float_as_uint(a) & 0x7F800000u;
-  const uint32_t emin = (uint32_t)(127 - 14) << 23;
-  e = (e < emin ? emin : e) - (10u << 23);
-  // a uniform fraction in [0, 1) from the top 23 bits of r: the float 1.f
-  // with those bits as its mantissa, minus 1 (exact)
-  const float f = __fsub_rn(__uint_as_float(0x3F800000u | (r >> 9)), 1.0f);
-  const float t = __fmaf_rn(f, __uint_as_float(e), a);
-  return (unsigned short)(__half_as_ushort(__float2half_rz(t)) | (sign >> 16));
+__device__ __forceinline__ uint32_t sr_pack_bf16x2(float hi, float lo, uint32_t r) {
+  uint32_t d;
+  asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(r));
+  return d;
 }
 
 }  // namespace cupf
