@@ -299,6 +299,8 @@ def serve_stream(prec, nreq, fix=None, device=0):
         shapes = [g for g in SERVE_GRIDS if any(c.meta["interior"] == g for _, c in reqs)]
         warm = [srv.submit(next(c for _, c in reqs if c.meta["interior"] == g), 5) for g in shapes]
         srv.run_until_done(warm)
+        # the autotuner's tile shape per grid shape: (column-tile height, z chunk)
+        tiles = {"x".join(map(str, g)): list(srv.tile(w)) for g, w in zip(shapes, warm)}
         for w in warm:
             srv.release(w)
         t0 = time.perf_counter()
@@ -365,7 +367,7 @@ def serve_stream(prec, nreq, fix=None, device=0):
         # the request's dynamics resolve)
         worst["results_fp64_perturbed_beyond_tolerance"] = sum(
             1 for e in errors if "fp64_perturbed" in e and not within_tol(e["fp64_perturbed"]))
-    return {"precision": prec, "sims_per_hr": len(res) / span * 3600.0,
+    return {"precision": prec, "tiles_autotuned": tiles, "sims_per_hr": len(res) / span * 3600.0,
             "p50_s": float(np.percentile(ttr, 50)), "p99_s": float(np.percentile(ttr, 99)),
             "mcell_upd_per_s": cells / span / 1e6, "requests": len(res),
             "arrival_rate_per_s": 4.0, "steps_per_request": SERVE_STEPS,

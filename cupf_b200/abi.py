@@ -46,7 +46,7 @@ class cupf_apt_inputs(C.Structure):
 class cupf_server_config(C.Structure):
     _fields_ = [("device", C.c_int32), ("precision", C.c_int32), ("num_pf", C.c_int32),
                 ("max_active", C.c_int32), ("steps_per_round", C.c_int32),
-                ("autotune", C.c_int32), ("hbm_budget_bytes", C.c_int64)]
+                ("autotune", C.c_int32), ("hbm_budget_bytes", C.c_int64), ("tile_y", C.c_int32)]
 
 
 class cupf_ek2d_params(C.Structure):
@@ -116,6 +116,7 @@ def lib():
             "cupf_apt_set_tuning": [vp, C.c_int32],
             "cupf_apt_set_skip_quiet": [vp, C.c_int32],
             "cupf_apt_set_wait_limit": [vp, C.c_int64],
+            "cupf_apt_set_tile": [vp, C.c_int32],
             "cupf_apt_active_cells": [vp, C.POINTER(C.c_uint64)],
             "cupf_apt_nucl_init": [vp],
             "cupf_apt_nucleate": [vp, C.c_int32, C.POINTER(C.c_int32)],
@@ -168,6 +169,9 @@ def lib():
                                    C.POINTER(C.c_int64), C.c_int32, C.POINTER(C.c_double),
                                    C.POINTER(C.c_double)],
             "cupf_server_release": [vp, C.c_int64],
+            "cupf_server_request_tile": [vp, C.c_int64, C.POINTER(C.c_int32),
+                                         C.POINTER(C.c_int32)],
+            "cupf_server_set_tile": [vp, C.c_int32],
             "cupf_server_stats": [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64)],
             "cupf_ek2d_derive": [C.POINTER(cupf_ek2d_params), C.c_float],
             "cupf_ek2d_parse_input": [C.c_char_p, C.POINTER(cupf_ek2d_params),

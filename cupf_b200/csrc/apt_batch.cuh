@@ -27,12 +27,14 @@ struct BatchSim {
   int pad;
 };
 
-template <int NP, class S>
-__global__ void __launch_bounds__(NTHREADS, step_min_blocks<NP, S>())
+// TY: the column-tile height of every simulation in the launch (the server
+// launches one kernel per tile height present in a round).
+template <int NP, class S, int TY>
+__global__ void __launch_bounds__(tile_threads<TY>(), step_min_blocks<NP, S, TY>())
     apt_batch_step_kernel(BatchSim* sims, const CUtensorMap* tmaps, const int4* items, int nitems,
                           int* work, const int* err) {
   extern __shared__ __align__(128) unsigned char smem[];
-  CtaSmem<NP, S> sm(smem);
+  CtaSmem<NP, S, TY> sm(smem);
   sm.init();
   int qbase = 0;
   for (;;) {
@@ -52,8 +54,8 @@ __global__ void __launch_bounds__(NTHREADS, step_min_blocks<NP, S>())
     a.t = __fmul_rn(__fmul_rn((float)(sd->steps + 1), a.dt), a.tau0);
     a.t64 = __dmul_rn(__dmul_rn((double)(sd->steps + 1), (double)a.dt), (double)a.tau0);
     a.sr_key = (uint32_t)(sd->steps + 1);
-    if (a.quiet_out && item_quiet(a, w.y, w.z, w.w)) continue;
-    step_item<NP, S>(tmaps + 2 * w.x + cur, a, w.y, w.z, w.w, sm, qbase);
+    if (a.quiet_out && item_quiet<TY>(a, w.y, w.z, w.w)) continue;
+    step_item<NP, S, TY>(tmaps + 2 * w.x + cur, a, w.y, w.z, w.w, sm, qbase);
   }
   sm.drain();
 }

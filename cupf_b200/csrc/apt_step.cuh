@@ -5,7 +5,9 @@
 // grain-id gather with the first-seen merge, per-slot anisotropic update.
 //
 // Work decomposition: a CTA owns a TX x TY column tile of interior (x, y) cells
-// and a z chunk of ZC planes; one thread per (x, y) column marches z.  Planes of
+// (TX = 32, one warp per tile row; TY = 8 or 4, a template parameter the host
+// picks per simulation, the server by timing) and a z chunk of ZC planes; one
+// thread per (x, y) column marches z.  Planes of
 // the input pair buffer (all NUM_PF slots, tile plus one-cell halo) stream into
 // shared memory through a ring of S stages filled by TMA
 // (cp.async.bulk.tensor.4d, one 4-D box {TX+2, TY+2, 1, NP} per plane) and
@@ -35,14 +37,20 @@
 namespace cupf {
 
 constexpr int TX = 32;
-constexpr int TY = 8;
-constexpr int NTHREADS = TX * TY;
-constexpr int BH = TY + 2;  // box height (cells); the box width is the storage format's kBW
 constexpr int STAGES = 5;
 
-template <int NP, class S>
+// Column-tile heights the step is built for (the box height is TY + 2 cells; the
+// box width is the storage format's kBW).
+constexpr bool tile_height_built(int ty) { return ty == 8 || ty == 4; }
+template <int TY>
+constexpr int tile_threads() {
+  return TX * TY;
+}
+
+template <int NP, class S, int TY>
 struct StepSmem {
   static constexpr int BW = S::kBW;
+  static constexpr int BH = TY + 2;
   static constexpr int BCELLS = BW * BH;
   static constexpr int kBoxBytes = NP * BCELLS * S::kBytes;      // bytes one TMA plane load delivers
   static constexpr int kStageBytes = (kBoxBytes + 127) & ~127;  // stage stride (TMA dst: 128 B aligned)
@@ -148,10 +156,10 @@ __device__ __forceinline__ void fence_proxy_async() {
 }
 
 // Per-CTA shared-memory state, carved from the dynamic allocation.
-template <int NP, class S>
+template <int NP, class S, int TY>
 struct CtaSmem {
   using P = typename S::T;
-  using Smem = StepSmem<NP, S>;
+  using Smem = StepSmem<NP, S, TY>;
   P* stages;
   uint16_t* masks;
   uint64_t* bars;
@@ -192,12 +200,13 @@ struct CtaSmem {
 // this item is sequence number qbase + q, which fixes its stage (mod STAGES)
 // and the mbarrier phase parity; every issued plane is waited exactly once, in
 // order, so the phases stay consistent across items.
-template <int NP, class S>
+template <int NP, class S, int TY>
 __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArgs& a, int txi,
-                                          int tyi, int zci, CtaSmem<NP, S>& sm, int& qbase) {
+                                          int tyi, int zci, CtaSmem<NP, S, TY>& sm, int& qbase) {
   using Map = CodeMap<NP>;
   static_assert(NP <= 8, "slot codes are 4-bit fields of one 32-bit word");
-  using Smem = StepSmem<NP, S>;
+  using Smem = StepSmem<NP, S, TY>;
+  constexpr int NTHREADS = tile_threads<TY>();
   using P = typename S::T;
   constexpr int BW = Smem::BW;
   constexpr int BCELLS = Smem::BCELLS;
@@ -547,6 +556,7 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
 // (flag bits 2 and 1; a halo plane maps to an arbitrary plane, so there the
 // whole item's bit 0).  Every cell of such an item would be written as the empty
 // pair again.
+template <int TY>
 __device__ __forceinline__ bool item_quiet(const StepArgs& a, int txi, int tyi, int zci) {
   const int per = a.ntx * a.nty;
   const int it = zci * per + tyi * a.ntx + txi;
@@ -598,18 +608,22 @@ __device__ __forceinline__ int next_work_item(int* work, int nitems, int* s_item
 // nearest the bottom (the solid, where cells carry the most grain ids in a
 // directional-solidification run) start first and the light liquid chunks fill
 // in behind them.
-// Resident CTAs per SM the step is compiled for: three where three CTAs' shared
-// memory fits (16-bit pairs, or FP32 up to NUM_PF = 5), else two.
-template <int NP, class S>
+// Resident CTAs per SM the step is compiled for.  32x8 tiles: three where three
+// CTAs' shared memory fits (16-bit pairs, or FP32 up to NUM_PF = 5), else two.
+// 32x4 tiles: twice that (the same registers per thread), or as many as their
+// shared memory fits on one SM (228 KB) when fewer.
+template <int NP, class S, int TY>
 constexpr int step_min_blocks() {
-  return StepSmem<NP, S>::kBytes <= 74 * 1024 ? 3 : 2;
+  constexpr int tall = StepSmem<NP, S, 8>::kBytes <= 74 * 1024 ? 3 : 2;
+  constexpr int by_smem = (228 * 1024) / StepSmem<NP, S, TY>::kBytes;
+  return TY == 8 ? tall : (2 * tall < by_smem ? 2 * tall : by_smem);
 }
 
-template <int NP, class S>
-__global__ void __launch_bounds__(NTHREADS, step_min_blocks<NP, S>())
+template <int NP, class S, int TY>
+__global__ void __launch_bounds__(tile_threads<TY>(), step_min_blocks<NP, S, TY>())
     apt_step_kernel(const __grid_constant__ CUtensorMap tmap, const StepArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
-  CtaSmem<NP, S> sm(smem);
+  CtaSmem<NP, S, TY> sm(smem);
   sm.init();
   const int per_chunk = a.ntx * a.nty;
   const int nitems = per_chunk * a.nzc;
@@ -619,8 +633,8 @@ __global__ void __launch_bounds__(NTHREADS, step_min_blocks<NP, S>())
     if (it < 0) break;
     const int zci = it / per_chunk;
     const int r = it - zci * per_chunk;
-    if (a.quiet_out && item_quiet(a, r % a.ntx, r / a.ntx, zci)) continue;
-    step_item<NP, S>(&tmap, a, r % a.ntx, r / a.ntx, zci, sm, qbase);
+    if (a.quiet_out && item_quiet<TY>(a, r % a.ntx, r / a.ntx, zci)) continue;
+    step_item<NP, S, TY>(&tmap, a, r % a.ntx, r / a.ntx, zci, sm, qbase);
   }
   sm.drain();
 }

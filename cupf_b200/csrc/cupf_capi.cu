@@ -125,6 +125,7 @@ struct cupf_apt_handle {
   int counts_cap = 0;
   // launch shape
   int zc = 64;
+  int ty = 8;  // column-tile height (cupf_apt_set_tile)
   int ntx = 0, nty = 0, nzc = 0;
   // events for timing
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -180,7 +181,7 @@ static cupf_status make_tmap(cupf_apt_handle* h, int b) {
                           (cuuint64_t)g.np};
     cuuint64_t strides[3] = {(cuuint64_t)g.xp * e, (cuuint64_t)g.xp * g.fny * e,
                              (cuuint64_t)g.ss * e};
-    cuuint32_t box[4] = {(cuuint32_t)S::kBW, (cuuint32_t)BH, 1u, (cuuint32_t)g.np};
+    cuuint32_t box[4] = {(cuuint32_t)S::kBW, (cuuint32_t)(h->ty + 2), 1u, (cuuint32_t)g.np};
     cuuint32_t es[4] = {1, 1, 1, 1};
     CUresult r = enc(&h->tmap[b], S::kTmaType, 4, h->buf[b], dims, strides, box, es,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -209,24 +210,25 @@ static void free_handle(cupf_apt_handle* h) {
 }
 
 // ------------------------------------------------------------------ step launch
-template <int NP, class S>
+template <int NP, class S, int TY>
 static cupf_status launch_step_np(cupf_apt_handle* h, const StepArgs& a, const CUtensorMap& m) {
   static bool configured[64] = {};
   static int resident[64] = {};
-  const int bytes = StepSmem<NP, S>::kBytes;
+  constexpr int NTHREADS = tile_threads<TY>();
+  const int bytes = StepSmem<NP, S, TY>::kBytes;
   if (!configured[h->device & 63]) {
-    CK(cudaFuncSetAttribute(apt_step_kernel<NP, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            bytes));
+    CK(cudaFuncSetAttribute(apt_step_kernel<NP, S, TY>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     int per_sm = 0, nsm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, apt_step_kernel<NP, S>, NTHREADS,
-                                                     bytes));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, apt_step_kernel<NP, S, TY>,
+                                                     NTHREADS, bytes));
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
     resident[h->device & 63] = std::max(1, per_sm) * nsm;
     configured[h->device & 63] = true;
   }
   const int nitems = h->ntx * h->nty * h->nzc;
   const int nblk = std::min(nitems, h->grid_cap > 0 ? h->grid_cap : resident[h->device & 63]);
-  apt_step_kernel<NP, S><<<nblk, NTHREADS, bytes, h->stream>>>(m, a);
+  apt_step_kernel<NP, S, TY><<<nblk, NTHREADS, bytes, h->stream>>>(m, a);
   CK(cudaGetLastError());
   return CUPF_OK;
 }
@@ -235,9 +237,9 @@ static cupf_status launch_step(cupf_apt_handle* h, const StepArgs& a, const CUte
   return with_storage(h->prec, [&](auto tag) -> cupf_status {
     using S = decltype(tag);
     switch (h->g.np) {
-#define CASE(N) \
-  case N:       \
-    return launch_step_np<N, S>(h, a, m);
+#define CASE(N)                                                                 \
+  case N:                                                                       \
+    return h->ty == 4 ? launch_step_np<N, S, 4>(h, a, m) : launch_step_np<N, S, 8>(h, a, m);
       CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8)
 #undef CASE
       default:
@@ -313,7 +315,7 @@ static void set_zc(cupf_apt_handle* h, int zc) {
   const int nz = h->p.fnz - 2;
   h->zc = zc < 1 ? 1 : (zc > nz ? nz : zc);
   h->ntx = (h->p.fnx - 2 + TX - 1) / TX;
-  h->nty = (h->p.fny - 2 + TY - 1) / TY;
+  h->nty = (h->p.fny - 2 + h->ty - 1) / h->ty;
   h->nzc = (nz + h->zc - 1) / h->zc;
 }
 
@@ -331,9 +333,9 @@ static int resident_per_sm(const cupf_apt_handle* h) {
   with_storage(h->prec, [&](auto tag) -> cupf_status {
     using S = decltype(tag);
     switch (h->g.np) {
-#define CASE(N)                          \
-  case N:                                \
-    r = step_min_blocks<N, S>();         \
+#define CASE(N)                                                                      \
+  case N:                                                                            \
+    r = h->ty == 4 ? step_min_blocks<N, S, 4>() : step_min_blocks<N, S, 8>();        \
     break;
       CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8)
 #undef CASE
@@ -353,7 +355,8 @@ static int resident_per_sm(const cupf_apt_handle* h) {
 static int default_zc(cupf_apt_handle* h) {
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
-  const long long tiles = (long long)((h->p.fnx - 2 + TX - 1) / TX) * ((h->p.fny - 2 + TY - 1) / TY);
+  const long long tiles =
+      (long long)((h->p.fnx - 2 + TX - 1) / TX) * ((h->p.fny - 2 + h->ty - 1) / h->ty);
   const int nz = h->p.fnz - 2;
   const long long want = (5LL * resident_per_sm(h) * nsm + 1) / 2;
   for (int zc = 16; zc > 1; zc /= 2)
@@ -371,7 +374,8 @@ static int default_zc(cupf_apt_handle* h) {
 static int zc_for_active(cupf_apt_handle* h, int nz_active) {
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
-  const long long tiles = (long long)((h->p.fnx - 2 + TX - 1) / TX) * ((h->p.fny - 2 + TY - 1) / TY);
+  const long long tiles =
+      (long long)((h->p.fnx - 2 + TX - 1) / TX) * ((h->p.fny - 2 + h->ty - 1) / h->ty);
   const long long want = 2LL * resident_per_sm(h) * nsm;
   for (int zc = 16; zc > 1; zc /= 2)
     if (tiles * ((nz_active + zc - 1) / zc) >= want) return zc;
@@ -501,7 +505,8 @@ extern "C" cupf_status cupf_apt_create(const cupf_apt_params* p, const cupf_apt_
   TRY(cuda(cudaMemsetAsync(h->err, 0, sizeof(int), h->stream), "memset"));
   TRY(cuda(cudaMalloc((void**)&h->work, 2 * sizeof(int)), "work"));
   TRY(cuda(cudaMemsetAsync(h->work, 0, 2 * sizeof(int), h->stream), "memset"));
-  h->quiet_cap = (size_t)((p->fnx - 2 + TX - 1) / TX) * ((p->fny - 2 + TY - 1) / TY) * (p->fnz - 2);
+  // flags for the most items any tile height gives (32x4 tiles, z chunks of 1)
+  h->quiet_cap = (size_t)((p->fnx - 2 + TX - 1) / TX) * ((p->fny - 2 + 4 - 1) / 4) * (p->fnz - 2);
   for (int b = 0; b < 2; ++b) {
     TRY(cuda(cudaMalloc((void**)&h->quiet[b], h->quiet_cap), "quiet flags"));
     TRY(cuda(cudaMemsetAsync(h->quiet[b], 0, h->quiet_cap, h->stream), "memset"));
@@ -535,6 +540,20 @@ extern "C" cupf_status cupf_apt_set_tuning(cupf_apt_handle* h, int32_t z_chunk) 
   CK(cudaSetDevice(h->device));
   set_zc(h, z_chunk);
   h->zc_user = true;
+  return invalidate_quiet(h);
+}
+
+extern "C" cupf_status cupf_apt_set_tile(cupf_apt_handle* h, int32_t tile_y) {
+  if (!h) return fail(CUPF_ERR_INVALID, "null handle");
+  if (!tile_height_built(tile_y)) return fail(CUPF_ERR_INVALID, "tile_y must be 8 or 4");
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));  // no step in flight reads the old maps
+  h->ty = tile_y;
+  for (int b = 0; b < 2; ++b) {
+    const cupf_status e = make_tmap(h, b);
+    if (e) return e;
+  }
+  set_zc(h, h->zc);
   return invalidate_quiet(h);
 }
 
@@ -911,7 +930,7 @@ static NuclArgs nucl_args(cupf_apt_handle* h, int use_iuc) {
   a.count = h->nucl_count;
   a.quiet = h->quiet[h->cur];
   a.tw = TX;
-  a.th = TY;
+  a.th = h->ty;
   a.zc = h->zc;
   a.ntx = h->ntx;
   a.nty = h->nty;

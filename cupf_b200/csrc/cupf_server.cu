@@ -80,7 +80,7 @@ struct Request {
   float* ddummy = nullptr;
   uint8_t* dquiet[2] = {nullptr, nullptr};  // quiet-item flags of each buffer
   size_t bytes = 0;
-  int zc = 64, ntx = 0, nty = 0, nzc = 0;
+  int zc = 64, ty = 8, ntx = 0, nty = 0, nzc = 0;
   // results
   std::vector<int> res_alpha;
   std::vector<long long> res_volumes;
@@ -113,7 +113,8 @@ struct cupf_server {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   bool dirty = true;
-  std::map<std::tuple<int, int, int>, int> zc_cache;  // (fnx, fny, fnz) -> z chunk
+  // (fnx, fny, fnz) -> (tile height, z chunk)
+  std::map<std::tuple<int, int, int>, std::pair<int, int>> tile_cache;
   int64_t steps_replayed = 0;
   // device time of the rounds: events around each graph launch, summed when the
   // next pump has waited for it
@@ -154,17 +155,20 @@ static size_t request_bytes(const cupf_apt_params& p, int pair_bytes, int num_pf
   const int palign = pair_bytes == 8 ? 2 : 4;
   const size_t xp = (p.fnx + palign - 1) / palign * palign;
   const size_t L = (size_t)p.fnx * p.fny * p.fnz;
-  const size_t quiet = 2 * (size_t)((p.fnx - 2 + TX - 1) / TX) * ((p.fny - 2 + TY - 1) / TY) * (p.fnz - 2);
+  // quiet flags for the most items a tile shape gives (32x4 tiles, z chunks of 1)
+  const size_t quiet = 2 * (size_t)((p.fnx - 2 + TX - 1) / TX) * ((p.fny - 2 + 4 - 1) / 4) * (p.fnz - 2);
   return 2 * xp * p.fny * p.fnz * num_pf * pair_bytes + L * 8 + quiet + 4096;
 }
 
-// Pick the z chunk of a grid shape by timing the single-simulation step on a
-// scratch handle (same shape, precision, slot count) for a few chunk depths.
-static int autotune_zc(cupf_server* s, const Request* r) {
+// Pick the work items' tile shape of a grid shape -- the column-tile height
+// (32x8 or 32x4) and the z chunk -- by timing the single-simulation step on a
+// scratch handle (same shape, precision, slot count) for each candidate.
+static std::pair<int, int> autotune_tile(cupf_server* s, const Request* r) {
   const auto key = std::make_tuple(r->p.fnx, r->p.fny, r->p.fnz);
-  auto it = s->zc_cache.find(key);
-  if (it != s->zc_cache.end()) return it->second;
-  int best = 64;
+  auto it = s->tile_cache.find(key);
+  if (it != s->tile_cache.end()) return it->second;
+  const int fixed_ty = s->cfg.tile_y;
+  std::pair<int, int> best(fixed_ty ? fixed_ty : 8, 64);
   if (s->cfg.autotune) {
     cupf_apt_inputs in;
     std::memset(&in, 0, sizeof(in));
@@ -179,28 +183,32 @@ static int autotune_zc(cupf_server* s, const Request* r) {
     cupf_apt_handle* h = nullptr;
     if (cupf_apt_create(&r->p, &in, s->cfg.device, (cupf_precision)s->cfg.precision, &h) ==
         CUPF_OK) {
-      for (int zc : cand) {
-        if (zc > 2 * nz && zc != cand[0]) break;
-        // the fastest of three timings of 4 steps, after 2 untimed ones (a single
-        // short timing picked different chunks from run to run)
-        float ms = 1e30f;
-        bool ok = cupf_apt_set_tuning(h, zc) == CUPF_OK &&
-                  cupf_apt_init_from_argmax(h, r->phi.data(), r->alpha.data()) == CUPF_OK &&
-                  cupf_apt_step(h, 2, 0) == CUPF_OK;
-        for (int rep = 0; ok && rep < 3; ++rep) {
-          float m = 0;
-          ok = cupf_apt_time_steps(h, 4, &m) == CUPF_OK;
-          ms = std::min(ms, m);
-        }
-        if (ok && ms < best_ms) {
-          best_ms = ms;
-          best = zc;
+      for (int ty : {8, 4}) {
+        if (fixed_ty && ty != fixed_ty) continue;
+        if (cupf_apt_set_tile(h, ty) != CUPF_OK) continue;
+        for (int zc : cand) {
+          if (zc > 2 * nz && zc != cand[0]) break;
+          // the fastest of three timings of 4 steps, after 2 untimed ones (a
+          // single short timing picked different chunks from run to run)
+          float ms = 1e30f;
+          bool ok = cupf_apt_set_tuning(h, zc) == CUPF_OK &&
+                    cupf_apt_init_from_argmax(h, r->phi.data(), r->alpha.data()) == CUPF_OK &&
+                    cupf_apt_step(h, 2, 0) == CUPF_OK;
+          for (int rep = 0; ok && rep < 3; ++rep) {
+            float m = 0;
+            ok = cupf_apt_time_steps(h, 4, &m) == CUPF_OK;
+            ms = std::min(ms, m);
+          }
+          if (ok && ms < best_ms) {
+            best_ms = ms;
+            best = std::make_pair(ty, zc);
+          }
         }
       }
       cupf_apt_destroy(h);
     }
   }
-  s->zc_cache[key] = best;
+  s->tile_cache[key] = best;
   return best;
 }
 
@@ -214,11 +222,13 @@ static cupf_status admit(cupf_server* s, Request* r, int slot) {
   r->g.np = np;
   r->g.xp = (p.fnx + palign - 1) / palign * palign;
   r->g.ss = (long long)r->g.xp * p.fny * p.fnz;
-  r->zc = autotune_zc(s, r);
+  const std::pair<int, int> tile = autotune_tile(s, r);
+  r->ty = tile.first;
+  r->zc = tile.second;
   const int nz = p.fnz - 2;
   r->zc = std::min(r->zc, nz);
   r->ntx = (p.fnx - 2 + TX - 1) / TX;
-  r->nty = (p.fny - 2 + TY - 1) / TY;
+  r->nty = (p.fny - 2 + r->ty - 1) / r->ty;
   r->nzc = (nz + r->zc - 1) / r->zc;
   const size_t bb = (size_t)r->g.ss * np * s->pair_bytes;
   const size_t L = (size_t)p.fnx * p.fny * p.fnz;
@@ -274,7 +284,7 @@ static cupf_status admit(cupf_server* s, Request* r, int slot) {
                             (cuuint64_t)np};
       cuuint64_t strides[3] = {(cuuint64_t)r->g.xp * eb, (cuuint64_t)r->g.xp * p.fny * eb,
                                (cuuint64_t)r->g.ss * eb};
-      cuuint32_t box[4] = {(cuuint32_t)S::kBW, (cuuint32_t)BH, 1u, (cuuint32_t)np};
+      cuuint32_t box[4] = {(cuuint32_t)S::kBW, (cuuint32_t)(r->ty + 2), 1u, (cuuint32_t)np};
       cuuint32_t es[4] = {1, 1, 1, 1};
       if (enc(&tm[b], S::kTmaType, 4, r->buf[b], dims, strides, box, es,
               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -420,15 +430,28 @@ static cupf_status retire(cupf_server* s, Request* r, int cur) {
   return CUPF_OK;
 }
 
+// Work items of every resident simulation, grouped by tile height (32x8 first,
+// then 32x4): per step one persistent batched launch per group present, each
+// with its own range of the item list and its own work counter, then the
+// finish kernel.
+static const int kTileHeights[2] = {8, 4};
+
 static cupf_status rebuild(cupf_server* s) {
   std::vector<int4> items;
-  for (size_t slot = 0; slot < s->slots.size(); ++slot) {
-    if (!s->slots[slot]) continue;
-    const Request* r = s->reqs[s->slots[slot]].get();
-    for (int tyi = 0; tyi < r->nty; ++tyi)
-      for (int txi = 0; txi < r->ntx; ++txi)
-        for (int zci = 0; zci < r->nzc; ++zci) items.push_back(make_int4((int)slot, txi, tyi, zci));
+  int off[3] = {0, 0, 0};
+  for (int gi = 0; gi < 2; ++gi) {
+    off[gi] = (int)items.size();
+    for (size_t slot = 0; slot < s->slots.size(); ++slot) {
+      if (!s->slots[slot]) continue;
+      const Request* r = s->reqs[s->slots[slot]].get();
+      if (r->ty != kTileHeights[gi]) continue;
+      for (int tyi = 0; tyi < r->nty; ++tyi)
+        for (int txi = 0; txi < r->ntx; ++txi)
+          for (int zci = 0; zci < r->nzc; ++zci)
+            items.push_back(make_int4((int)slot, txi, tyi, zci));
+    }
   }
+  off[2] = (int)items.size();
   s->nitems = (int)items.size();
   if (s->nitems > s->items_cap) {
     if (s->d_items) cudaFree(s->d_items);
@@ -438,7 +461,7 @@ static cupf_status rebuild(cupf_server* s) {
   if (s->nitems)
     CK(cudaMemcpyAsync(s->d_items, items.data(), items.size() * sizeof(int4),
                        cudaMemcpyHostToDevice, s->stream));
-  CK(cudaMemsetAsync(s->d_next, 0, 2 * sizeof(int), s->stream));
+  CK(cudaMemsetAsync(s->d_next, 0, 4 * sizeof(int), s->stream));
   if (s->gexec) {
     cudaGraphExecDestroy(s->gexec);
     s->gexec = nullptr;
@@ -451,30 +474,44 @@ static cupf_status rebuild(cupf_server* s) {
     s->dirty = false;
     return CUPF_OK;
   }
-  // persistent grid: the resident CTAs of the step kernel, never more than items
+  // persistent grids: the resident CTAs of each step kernel, never more than items
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, s->cfg.device);
   const int nsims = (int)s->slots.size();
   cupf_status e = with_fmt(s->cfg.precision, [&](auto tag) -> cupf_status {
     using S = decltype(tag);
     switch (s->cfg.num_pf) {
-#define CASE(N)                                                                              \
-  case N: {                                                                                  \
-    const int bytes = StepSmem<N, S>::kBytes;                                                \
-    CK(cudaFuncSetAttribute(apt_batch_step_kernel<N, S>,                                     \
-                            cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));            \
-    int per_sm = 2;                                                                          \
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, apt_batch_step_kernel<N, S>,   \
-                                                     NTHREADS, bytes));                      \
-    const int grid = std::min(s->nitems, std::max(1, per_sm) * nsm);                         \
-    CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));                 \
-    for (int k = 0; k < s->cfg.steps_per_round; ++k) {                                       \
-      apt_batch_step_kernel<N, S><<<grid, NTHREADS, bytes, s->stream>>>(                     \
-          s->d_sims, s->d_tmaps, s->d_items, s->nitems, s->d_next, s->d_err);                \
-      batch_finish_kernel<<<(nsims + 127) / 128, 128, 0, s->stream>>>(s->d_sims, nsims);     \
-    }                                                                                        \
-    CK(cudaStreamEndCapture(s->stream, &s->graph));                                          \
-    return CUPF_OK;                                                                          \
+#define CASE(N)                                                                                 \
+  case N: {                                                                                     \
+    int grid[2] = {0, 0};                                                                       \
+    const int bytes8 = StepSmem<N, S, 8>::kBytes, bytes4 = StepSmem<N, S, 4>::kBytes;           \
+    CK(cudaFuncSetAttribute(apt_batch_step_kernel<N, S, 8>,                                     \
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, bytes8));              \
+    CK(cudaFuncSetAttribute(apt_batch_step_kernel<N, S, 4>,                                     \
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, bytes4));              \
+    for (int gi = 0; gi < 2; ++gi) {                                                            \
+      int per_sm = 2;                                                                           \
+      if (gi == 0)                                                                              \
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(                                       \
+            &per_sm, apt_batch_step_kernel<N, S, 8>, tile_threads<8>(), bytes8));               \
+      else                                                                                      \
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(                                       \
+            &per_sm, apt_batch_step_kernel<N, S, 4>, tile_threads<4>(), bytes4));               \
+      grid[gi] = std::min(off[gi + 1] - off[gi], std::max(1, per_sm) * nsm);                    \
+    }                                                                                           \
+    CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));                    \
+    for (int k = 0; k < s->cfg.steps_per_round; ++k) {                                          \
+      if (grid[0] > 0)                                                                          \
+        apt_batch_step_kernel<N, S, 8><<<grid[0], tile_threads<8>(), bytes8, s->stream>>>(      \
+            s->d_sims, s->d_tmaps, s->d_items + off[0], off[1] - off[0], s->d_next, s->d_err);  \
+      if (grid[1] > 0)                                                                          \
+        apt_batch_step_kernel<N, S, 4><<<grid[1], tile_threads<4>(), bytes4, s->stream>>>(      \
+            s->d_sims, s->d_tmaps, s->d_items + off[1], off[2] - off[1], s->d_next + 2,         \
+            s->d_err);                                                                          \
+      batch_finish_kernel<<<(nsims + 127) / 128, 128, 0, s->stream>>>(s->d_sims, nsims);        \
+    }                                                                                           \
+    CK(cudaStreamEndCapture(s->stream, &s->graph));                                             \
+    return CUPF_OK;                                                                             \
   }
       CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8)
 #undef CASE
@@ -496,6 +533,8 @@ extern "C" cupf_status cupf_server_create(const cupf_server_config* cfg, cupf_se
   if (cfg->max_active < 1 || cfg->max_active > 4096)
     return cupf_fail(CUPF_ERR_INVALID, "max_active must be in 1..4096");
   if (cfg->steps_per_round < 1) return cupf_fail(CUPF_ERR_INVALID, "steps_per_round must be >= 1");
+  if (cfg->tile_y != 0 && !tile_height_built(cfg->tile_y))
+    return cupf_fail(CUPF_ERR_INVALID, "tile_y must be 0, 4 or 8");
   if (cfg->precision < 0 || cfg->precision > 2)
     return cupf_fail(CUPF_ERR_UNSUPPORTED, "precision %d", cfg->precision);
   std::unique_ptr<cupf_server> s(new cupf_server());
@@ -509,8 +548,8 @@ extern "C" cupf_status cupf_server_create(const cupf_server_config* cfg, cupf_se
   CK(cudaMalloc((void**)&s->d_sims, cfg->max_active * sizeof(BatchSim)));
   CK(cudaMemset(s->d_sims, 0, cfg->max_active * sizeof(BatchSim)));
   CK(cudaMalloc((void**)&s->d_tmaps, 2 * cfg->max_active * sizeof(CUtensorMap)));
-  CK(cudaMalloc((void**)&s->d_next, 2 * sizeof(int)));
-  CK(cudaMemset(s->d_next, 0, 2 * sizeof(int)));
+  CK(cudaMalloc((void**)&s->d_next, 4 * sizeof(int)));  // a work counter pair per tile height
+  CK(cudaMemset(s->d_next, 0, 4 * sizeof(int)));
   CK(cudaMalloc((void**)&s->d_err, sizeof(int)));
   CK(cudaMemset(s->d_err, 0, sizeof(int)));
   CK(cudaMalloc((void**)&s->d_part, 2 * 148 * 4 * sizeof(double)));
@@ -677,6 +716,27 @@ extern "C" cupf_status cupf_server_stats(cupf_server* s, double* busy_ms, int64_
   if (!s) return cupf_fail(CUPF_ERR_INVALID, "null server");
   if (busy_ms) *busy_ms = s->busy_ms;
   if (rounds) *rounds = s->steps_replayed / std::max(1, (int)s->cfg.steps_per_round);
+  return CUPF_OK;
+}
+
+extern "C" cupf_status cupf_server_request_tile(cupf_server* s, int64_t id, int32_t* tile_y,
+                                                int32_t* z_chunk) {
+  if (!s) return cupf_fail(CUPF_ERR_INVALID, "null server");
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return cupf_fail(CUPF_ERR_INVALID, "unknown request");
+  const Request* r = it->second.get();
+  const bool placed = r->state != PENDING;
+  if (tile_y) *tile_y = placed ? r->ty : 0;
+  if (z_chunk) *z_chunk = placed ? r->zc : 0;
+  return CUPF_OK;
+}
+
+extern "C" cupf_status cupf_server_set_tile(cupf_server* s, int32_t tile_y) {
+  if (!s) return cupf_fail(CUPF_ERR_INVALID, "null server");
+  if (tile_y != 0 && !tile_height_built(tile_y))
+    return cupf_fail(CUPF_ERR_INVALID, "tile_y must be 0, 4 or 8");
+  s->cfg.tile_y = tile_y;
+  s->tile_cache.clear();
   return CUPF_OK;
 }
 

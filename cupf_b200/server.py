@@ -39,10 +39,13 @@ def poisson_stream(n, seed=0, num_pf=8, rate=4.0):
 
 class Server:
     def __init__(self, device=0, precision="fp32", num_pf=8, max_active=64, steps_per_round=50,
-                 autotune=True, hbm_budget_bytes=0):
+                 autotune=True, hbm_budget_bytes=0, tile_y=0):
+        """tile_y: 0 lets the autotuner pick each grid shape's column-tile height
+        with its z chunk (8 without autotune); 4 or 8 fixes it."""
         self.L = abi.lib()
         cfg = abi.cupf_server_config(device, abi.PREC[precision], num_pf, max_active,
-                                     steps_per_round, int(bool(autotune)), int(hbm_budget_bytes))
+                                     steps_per_round, int(bool(autotune)), int(hbm_budget_bytes),
+                                     int(tile_y))
         h = C.c_void_p()
         abi.check(self.L.cupf_server_create(C.byref(cfg), C.byref(h)))
         self.h = h
@@ -107,6 +110,19 @@ class Server:
         n = C.c_int64()
         abi.check(self.L.cupf_server_stats(self.h, C.byref(ms), C.byref(n)))
         return ms.value, n.value
+
+    def tile(self, rid):
+        """(column-tile height, z chunk) of an admitted request ((0, 0) before)."""
+        ty, zc = C.c_int32(), C.c_int32()
+        abi.check(self.L.cupf_server_request_tile(self.h, rid, C.byref(ty), C.byref(zc)))
+        return ty.value, zc.value
+
+    def tile_height(self, rid):
+        return self.tile(rid)[0]
+
+    def set_tile_height(self, tile_y):
+        """Tile height of requests admitted from now on (0 = autotuned)."""
+        abi.check(self.L.cupf_server_set_tile(self.h, int(tile_y)))
 
     def release(self, rid):
         abi.check(self.L.cupf_server_release(self.h, rid))

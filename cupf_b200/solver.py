@@ -154,6 +154,10 @@ class APTSolver:
     def set_tuning(self, z_chunk):
         abi.check(self.L.cupf_apt_set_tuning(self.h, int(z_chunk)))
 
+    def set_tile(self, tile_y):
+        """Column-tile height of the step's work items: 8 (default) or 4."""
+        abi.check(self.L.cupf_apt_set_tile(self.h, int(tile_y)))
+
     def set_wait_limit(self, cycles):
         """Bound of the step's plane-load waits in SM cycles (0 = default, ~1 s)."""
         abi.check(self.L.cupf_apt_set_wait_limit(self.h, int(cycles)))

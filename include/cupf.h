@@ -308,6 +308,12 @@ void* cupf_apt_stream(cupf_apt_handle* h);
  * planes that hold grain ids; after it, the given chunk stays. */
 cupf_status cupf_apt_set_tuning(cupf_apt_handle* h, int32_t z_chunk);
 
+/* Column-tile height of the step's work items (no counterpart in the reference,
+ * whose kernel uses 32x4 thread blocks): 8 (the default) or 4 rows of 32 cells.
+ * Results are identical for both; only the speed differs (the server picks per
+ * grid shape by timing both with the z chunk).  Resets the quiet-item flags. */
+cupf_status cupf_apt_set_tile(cupf_apt_handle* h, int32_t tile_y);
+
 /* Quiet work items (on by default).  The step keeps, per work item and buffer, a
  * flag that every slot of the item's cells holds the empty pair (id -1, phi -1),
  * and leaves an item alone when its cells in the buffer it writes are already
@@ -351,8 +357,10 @@ typedef struct cupf_server_config {
   int32_t num_pf;           /* NUM_PF, shared by every request */
   int32_t max_active;       /* resident simulations at most */
   int32_t steps_per_round;  /* steps per graph replay (one pump) */
-  int32_t autotune;         /* 1: pick the z chunk of each grid shape by timing */
+  int32_t autotune;         /* 1: pick the tile height and z chunk of each grid shape by timing */
   int64_t hbm_budget_bytes; /* device memory for requests; 0 = free memory - 2 GiB */
+  int32_t tile_y;           /* column-tile height: 0 = the autotuner's pick (8 without
+                               autotune), or 4 / 8 for every request */
 } cupf_server_config;
 
 cupf_status cupf_server_create(const cupf_server_config* cfg, cupf_server** out);
@@ -389,6 +397,17 @@ cupf_status cupf_server_result(cupf_server* s, int64_t id, int32_t* status, int3
 
 /* Forget a finished (or still queued) request and its host results. */
 cupf_status cupf_server_release(cupf_server* s, int64_t id);
+
+/* Tile shape of a request's work items: the column-tile height (8 or 4) and the
+ * z chunk the autotuner (or the configuration) picked for its grid shape; 0 and
+ * 0 until it is admitted.  Either output pointer may be NULL. */
+cupf_status cupf_server_request_tile(cupf_server* s, int64_t id, int32_t* tile_y,
+                                     int32_t* z_chunk);
+
+/* Column-tile height of requests admitted from now on: 0 = the autotuner's pick
+ * (8 without autotune), 4 or 8 fixed (as cupf_server_config::tile_y).  Forgets
+ * the earlier picks; resident requests keep theirs. */
+cupf_status cupf_server_set_tile(cupf_server* s, int32_t tile_y);
 
 #ifdef __cplusplus
 }
