@@ -437,15 +437,16 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
       return S::phi(pts[s][cd * BCELLS]);
     };
 
-    // center values of every slot (for the repulsion sum); the loops over slots
-    // stop at n, so a warp runs only as many iterations as its fullest cell
-    float phc[NP];
+    // phi + 1 at the centre for every slot (the repulsion sum's terms); the loops
+    // over slots stop at n, so a warp runs only as many iterations as its
+    // fullest cell
+    float phc1[NP];
 #pragma unroll
-    for (int q = 0; q < NP; ++q) phc[q] = -1.0f;
+    for (int q = 0; q < NP; ++q) phc1[q] = 0.0f;
 #pragma unroll
     for (int q = 0; q < NP; ++q) {
       if (q >= n) break;
-      phc[q] = fetch(3, q);
+      phc1[q] = __fadd_rn(fetch(3, q), 1.0f);
     }
 
     // rounding bits of this cell and step: keyed on the cell's reference-layout
@@ -483,12 +484,21 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
         sinb = t_o.z;
         cosb = t_o.w;
       }
-      float repul = 0.0f;
+      // repulsion sum over the other slots (APTPhaseField.cu:328-335): the
+      // reference accumulates r += 0.25 (phi+1)(phi+1) with the product fused,
+      // r' = RN(0.25 q q + r).  Kept four times larger, R = 4 r, the same sum is
+      // R' = RN(q q + R) = 4 RN(0.25 q q + r) exactly (scaling by a power of two
+      // commutes with rounding; every term is far from the subnormal range), so
+      // one fused multiply-add per term and one multiply at the end give the
+      // reference's bits.
+      static_assert(Contract::REP == 1, "the scaled sum restates the fused form only");
+      float rsum = 0.0f;
 #pragma unroll
       for (int q = 0; q < NP; ++q) {
         if (q >= n) break;
-        if (q != j) repul = repul_add(repul, phc[q]);
+        if (q != j) rsum = __fmaf_rn(phc1[q], phc1[q], rsum);
       }
+      const float repul = __fmul_rn(0.25f, rsum);
       const float nv = slot_update(a, kc, ph7, sina, cosa, sinb, cosb, repul, Up);
       const int oid = (nv < kDrop) ? -1 : id;  // (double)nv < -0.9999
       // slot j's rounding bits: the cell's hashed key times a distinct odd
