@@ -240,6 +240,10 @@ static __global__ void archive_kernel(const int* __restrict__ alpha, int* alpha_
 // Voxel count per grain id over the interior of the argmax map, plus the first
 // (k, j, i)-order index where each id occurs (for the reference's first-seen
 // ordering, QOI.cpp:198-231).  counts[0] = interior cells with no grain.
+// Neighbouring cells mostly share a grain, so the lanes of a warp holding the
+// same id add their count in one atomic from the lowest of them, which also
+// holds their smallest index (a warp's lanes take consecutive interior cells,
+// whose reference-layout indices increase with the lane).
 static __global__ void volume_kernel(const int* __restrict__ alpha, int fnx, int fny, int fnz, int ng,
                               unsigned long long* counts, long long* first) {
   const long long ni = fnx - 2, nj = fny - 2, nk = fnz - 2;
@@ -249,11 +253,11 @@ static __global__ void volume_kernel(const int* __restrict__ alpha, int fnx, int
     const long long i = 1 + idx % ni, j = 1 + (idx / ni) % nj, k = 1 + idx / (ni * nj);
     const long long C = k * fnx * fny + j * fnx + i;
     const int a = alpha[C];
-    if (a >= 1 && a <= ng) {
-      atomicAdd(counts + a, 1ull);
-      atomicMin(first + a, C);
-    } else {
-      atomicAdd(counts, 1ull);
+    const int key = (a >= 1 && a <= ng) ? a : 0;
+    const unsigned peers = __match_any_sync(__activemask(), key);
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) {
+      atomicAdd(counts + key, (unsigned long long)__popc(peers));
+      if (key) atomicMin(first + key, C);
     }
   }
 }

@@ -32,6 +32,10 @@ struct StepArgs {
   int bcX, bcY, bcZ;
   int ntx, nty, nzc, zc;  // tile grid and z-chunk length
   int num_theta, thermalType, use_iuc;
+  // num_theta as an invariant divisor (invariant_divisor): the orientation index
+  // of a nucleated id, id % num_theta + 1, without a divide instruction
+  uint32_t nt_magic;
+  int nt_sh1, nt_sh2;
   float t;
   // time and height coordinates in FP64 (fp64 != 0: 16-bit storage, whose long
   // runs keep time, the moving-domain offset and the thermal model's
@@ -67,6 +71,36 @@ struct StepArgs {
   unsigned long long* active_cells;  // cells of the computed items, accumulated (may be NULL)
   long long wait_limit;  // SM cycles a stage wait may spin before the step gives up
 };
+
+// Unsigned division by a divisor fixed for a launch, by a multiply and shifts
+// (T. Granlund and P. Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994, fig. 4.1): for 1 <= d < 2^31 and every 32-bit n,
+// n / d = (t + ((n - t) >> s1)) >> s2 with t = mulhi(m, n), where
+// l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1, s1 = min(l, 1) and
+// s2 = max(l - 1, 0).
+struct InvariantDivisor {
+  uint32_t m;
+  int s1, s2;
+};
+inline InvariantDivisor invariant_divisor(uint32_t d) {
+  InvariantDivisor v{0u, 0, 0};
+  if (d == 0) return v;
+  int l = 0;
+  while ((1ull << l) < d) ++l;
+  v.m = (uint32_t)((((1ull << 32) * ((1ull << l) - d)) / d) + 1);
+  v.s1 = l < 1 ? l : 1;
+  v.s2 = l > 1 ? l - 1 : 0;
+  return v;
+}
+__host__ __device__ __forceinline__ uint32_t div_invariant(uint32_t n, uint32_t m, int s1,
+                                                           int s2) {
+#ifdef __CUDA_ARCH__
+  const uint32_t t = __umulhi(m, n);
+#else
+  const uint32_t t = (uint32_t)(((unsigned long long)m * n) >> 32);
+#endif
+  return (t + ((n - t) >> s1)) >> s2;
+}
 
 // Boundary map of one coordinate (APTsetBC3D, APTPhaseField.cu:111-112,134-135,157-158):
 // no-flux mirrors about the first/last interior point, periodic wraps.

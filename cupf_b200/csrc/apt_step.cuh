@@ -470,7 +470,8 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
       // here (cupf_apt_set_slots rejects other negative ids) and the clamp only
       // keeps a corrupted id from reading outside the tables
       int tid2 = id;
-      if (id > a.num_theta) tid2 = (id % a.num_theta) + 1;
+      if (id > a.num_theta)  // id % num_theta + 1
+        tid2 = id - (int)div_invariant((uint32_t)id, a.nt_magic, a.nt_sh1, a.nt_sh2) * a.num_theta + 1;
       const bool tab_ok = (unsigned)tid2 <= (unsigned)a.num_theta;
       const int ti = tab_ok ? tid2 : 0;
       const float4 t_o = __ldg(a.orient + ti);  // {sint[ti], cost[ti], sint[ti+NG], cost[ti+NG]}

@@ -265,6 +265,12 @@ static StepArgs step_args(cupf_apt_handle* h, float t, int use_iuc) {
   a.nzc = h->nzc;
   a.zc = h->zc;
   a.num_theta = p.num_theta;
+  {
+    const InvariantDivisor dv = invariant_divisor((uint32_t)p.num_theta);
+    a.nt_magic = dv.m;
+    a.nt_sh1 = dv.s1;
+    a.nt_sh2 = dv.s2;
+  }
   a.thermalType = p.thermalType;
   a.use_iuc = use_iuc;
   a.t = t;

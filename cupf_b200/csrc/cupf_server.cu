@@ -311,6 +311,12 @@ static cupf_status admit(cupf_server* s, Request* r, int slot) {
   a.nzc = r->nzc;
   a.zc = r->zc;
   a.num_theta = p.num_theta;
+  {
+    const InvariantDivisor dv = invariant_divisor((uint32_t)p.num_theta);
+    a.nt_magic = dv.m;
+    a.nt_sh1 = dv.s1;
+    a.nt_sh2 = dv.s2;
+  }
   a.thermalType = p.thermalType;
   a.kin_delta = p.kin_delta;
   a.eps = p.eps;
