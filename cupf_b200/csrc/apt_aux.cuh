@@ -23,35 +23,58 @@ struct Grid {
 // record of its mapped interior source (each coordinate mapped independently,
 // = sequential z, y, x face fills of APTsetBC3D, APTPhaseField.cu:93-174).
 // Cells are enumerated face by face without repetition.
-template <class S>
-__global__ void fill_halo_kernel(typename S::T* buf, Grid g, int bcX, int bcY, int bcZ) {
+__host__ __device__ __forceinline__ long long halo_cells(const Grid& g) {
+  return 2ll * g.fnx * g.fny + 2ll * g.fnx * (g.fnz - 2) + 2ll * (g.fny - 2) * (g.fnz - 2);
+}
+
+// Halo cell idx (0 .. halo_cells-1): the two z planes, then the two y faces of
+// the interior planes, then the two x faces of the interior rows.
+__device__ __forceinline__ void halo_cell(long long idx, const Grid& g, int& i, int& j, int& k) {
   const long long nz2 = 2ll * g.fnx * g.fny;
   const long long ny2 = 2ll * g.fnx * (g.fnz - 2);
   const long long nx2 = 2ll * (g.fny - 2) * (g.fnz - 2);
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < nz2 + ny2 + nx2;
+  long long r = idx;
+  if (r < nz2) {
+    k = (r < nz2 / 2) ? 0 : g.fnz - 1;
+    r %= (long long)g.fnx * g.fny;
+    j = (int)(r / g.fnx);
+    i = (int)(r % g.fnx);
+  } else if ((r -= nz2) < ny2) {
+    j = (r < ny2 / 2) ? 0 : g.fny - 1;
+    r %= (long long)g.fnx * (g.fnz - 2);
+    k = 1 + (int)(r / g.fnx);
+    i = (int)(r % g.fnx);
+  } else {
+    r -= ny2;
+    i = (r < nx2 / 2) ? 0 : g.fnx - 1;
+    r %= (long long)(g.fny - 2) * (g.fnz - 2);
+    k = 1 + (int)(r / (g.fny - 2));
+    j = 1 + (int)(r % (g.fny - 2));
+  }
+}
+
+template <class S>
+__global__ void fill_halo_kernel(typename S::T* buf, Grid g, int bcX, int bcY, int bcZ) {
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < halo_cells(g);
        idx += (long long)gridDim.x * blockDim.x) {
     int i, j, k;
-    long long r = idx;
-    if (r < nz2) {
-      k = (r < nz2 / 2) ? 0 : g.fnz - 1;
-      r %= (long long)g.fnx * g.fny;
-      j = (int)(r / g.fnx);
-      i = (int)(r % g.fnx);
-    } else if ((r -= nz2) < ny2) {
-      j = (r < ny2 / 2) ? 0 : g.fny - 1;
-      r %= (long long)g.fnx * (g.fnz - 2);
-      k = 1 + (int)(r / g.fnx);
-      i = (int)(r % g.fnx);
-    } else {
-      r -= ny2;
-      i = (r < nx2 / 2) ? 0 : g.fnx - 1;
-      r %= (long long)(g.fny - 2) * (g.fnz - 2);
-      k = 1 + (int)(r / (g.fny - 2));
-      j = 1 + (int)(r % (g.fny - 2));
-    }
+    halo_cell(idx, g, i, j, k);
     const long long d = g.at(i, j, k);
     const long long s = g.at(bc_map(i, g.fnx, bcX), bc_map(j, g.fny, bcY), bc_map(k, g.fnz, bcZ));
     for (int p = 0; p < g.np; ++p) buf[p * g.ss + d] = buf[p * g.ss + s];
+  }
+}
+
+// The halo cells of every slot, copied from src to dst unchanged.
+template <class S>
+__global__ void copy_halo_kernel(const typename S::T* __restrict__ src, typename S::T* dst,
+                                 Grid g) {
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < halo_cells(g);
+       idx += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    halo_cell(idx, g, i, j, k);
+    const long long d = g.at(i, j, k);
+    for (int p = 0; p < g.np; ++p) dst[p * g.ss + d] = src[p * g.ss + d];
   }
 }
 

@@ -1038,6 +1038,18 @@ extern "C" cupf_status cupf_apt_move_domain(cupf_apt_handle* h, int32_t* tip_fro
     (*tip_front)++;
   *moved = 0;
   const long long plane = (long long)p.fnx * p.fny;
+  // Each layer moved: the argmax of the current buffer, its bottom interior layer
+  // archived, then the interior shifted down one plane into the other buffer
+  // (APTmove_frame), and copied back (APTcopy_frame: the interior only, so the
+  // halo the next layer's argmax reads is the one from before the move).  Where
+  // the thermal model updates every slot of every cell the step computes (types
+  // 0, 1, 2, 5), the next step overwrites the other buffer wherever it is not
+  // already empty, so instead of the copy back the halo cells go across and the
+  // buffers swap (the other keeps the state before the move).  The cone and
+  // paraboloid-table models (3, 4) leave slots unwritten past their fronts,
+  // which must then hold the moved state: there the copy back stays.
+  const int cur0 = h->cur;
+  const bool swap = p.thermalType != 3 && p.thermalType != 4;
   while (*tip_front >= tip_thres) {
     if (*move_count + 2 > h->fnz_f) {  // grow the archive
       const int nf = h->fnz_f * 2;
@@ -1057,8 +1069,14 @@ extern "C" cupf_status cupf_apt_move_domain(cupf_apt_handle* h, int32_t* tip_fro
                                                            p.fnx, p.fny, *move_count, p.num_theta);
     const long long ni = (long long)(p.fnx - 2) * (p.fny - 2) * (p.fnz - 2) * p.num_pf;
     LAUNCH_S(h, shift_kernel, grid_for(ni), 256, B<S>(h->buf[h->cur]), B<S>(h->buf[h->cur ^ 1]), g);
-    LAUNCH_S(h, copy_interior_kernel, grid_for(ni), 256, B<S>(h->buf[h->cur ^ 1]),
-             B<S>(h->buf[h->cur]), g);
+    if (swap) {
+      LAUNCH_S(h, copy_halo_kernel, grid_for(halo_cells(g)), 256, B<S>(h->buf[h->cur]),
+               B<S>(h->buf[h->cur ^ 1]), g);
+      h->cur ^= 1;
+    } else {
+      LAUNCH_S(h, copy_interior_kernel, grid_for(ni), 256, B<S>(h->buf[h->cur ^ 1]),
+               B<S>(h->buf[h->cur]), g);
+    }
     CK(cudaGetLastError());
     // z shift (APTmove_frame :365-369 then APTcopy_frame :401-402)
     std::vector<float>& z = h->z_host;
@@ -1079,18 +1097,25 @@ extern "C" cupf_status cupf_apt_move_domain(cupf_apt_handle* h, int32_t* tip_fro
     *moved += 1;
   }
   if (*moved) {
-    // both buffers now hold the shifted state: shift the current buffer's flags
-    // into the other one and copy them back
+    // quiet-item flags: the current buffer's are those of the state before the
+    // move shifted by the layers moved.  The other buffer holds the moved state
+    // too (copy back: the same flags), or the state before the move (swap, one
+    // layer: its flags unchanged), or an intermediate state (swap, more layers:
+    // flags cleared, nothing known).
     const int per = h->ntx * h->nty;
-    quiet_shift_kernel<<<grid_for((long long)per * h->nzc), 256, 0, h->stream>>>(
-        h->quiet[h->cur], h->quiet[h->cur ^ 1], per, h->nzc, h->zc, p.fnz, *moved);
-    CK(cudaMemcpyAsync(h->quiet[h->cur], h->quiet[h->cur ^ 1], (size_t)per * h->nzc,
-                       cudaMemcpyDeviceToDevice, h->stream));
+    const size_t nq = (size_t)per * h->nzc;
+    const int tmp = h->cur == cur0 ? cur0 ^ 1 : h->cur;
+    quiet_shift_kernel<<<grid_for((long long)nq), 256, 0, h->stream>>>(
+        h->quiet[cur0], h->quiet[tmp], per, h->nzc, h->zc, p.fnz, *moved);
+    if (tmp != h->cur)
+      CK(cudaMemcpyAsync(h->quiet[h->cur], h->quiet[tmp], nq, cudaMemcpyDeviceToDevice, h->stream));
+    if (swap && *moved > 1) CK(cudaMemsetAsync(h->quiet[h->cur ^ 1], 0, nq, h->stream));
     CK(cudaGetLastError());
   }
-  // both buffers hold the shifted interior: refill the halo of both
+  // the current buffer's halo still holds the state before the move (and so does
+  // the other's after a copy back)
   if ((st = fill_halo(h, h->cur))) return st;
-  if (*moved && (st = fill_halo(h, h->cur ^ 1))) return st;
+  if (*moved && !swap && (st = fill_halo(h, h->cur ^ 1))) return st;
   CK(cudaStreamSynchronize(h->stream));
   return check_err_word(h);
 }
