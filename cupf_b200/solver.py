@@ -142,8 +142,12 @@ class APTSolver:
     def nucl_init(self):
         abi.check(self.L.cupf_apt_nucl_init(self.h))
 
-    def nucleate(self, use_initial_undercooling=False):
-        """One nucleation pass; returns the number of nuclei so far."""
+    def nucleate(self, use_initial_undercooling=False, count=True):
+        """One nucleation pass; returns the number of nuclei so far (reading it
+        waits for the pass; count=False queues the pass and returns None)."""
+        if not count:
+            abi.check(self.L.cupf_apt_nucleate(self.h, int(bool(use_initial_undercooling)), None))
+            return None
         n = C.c_int32()
         abi.check(self.L.cupf_apt_nucleate(self.h, int(bool(use_initial_undercooling)), C.byref(n)))
         return n.value
