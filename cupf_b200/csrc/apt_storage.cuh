@@ -64,8 +64,11 @@ struct PairH16 {
   __device__ static float decode(unsigned short b) {
     const float c = (F == Half16::BF16) ? __bfloat162float(__ushort_as_bfloat16(b))
                                         : __half2float(__ushort_as_half(b));
+    // both bands as (c - s) k, s = sign of c: k = 1/K in the core, k = -1 in the
+    // tails (s - c exactly); the products are exact
     const float s = copysignf(1.0f, c);
-    return fabsf(c) >= 1.0f ? __fmul_rn(__fsub_rn(c, s), 1.0f / kCore) : __fsub_rn(s, c);
+    const float k = fabsf(c) >= 1.0f ? 1.0f / kCore : -1.0f;
+    return __fmul_rn(__fsub_rn(c, s), k);
   }
   // the FP32 value of the code before rounding to 16 bits
   __device__ static float code(float ph) {
