@@ -139,6 +139,7 @@ def lib():
                                             C.POINTER(C.c_int32), FP],
             "cupf_host_write_substrate": [C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_int32),
                                           C.c_int, FP],
+            "cupf_host_quaternions_to_angles": [C.c_int, C.POINTER(C.c_double), FP],
             "cupf_grain_volumes_noalloc": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                            C.POINTER(C.c_int64), vp],
             "cupf_dense_create": [C.POINTER(cupf_apt_params), C.POINTER(cupf_apt_inputs), C.c_float,

@@ -1,5 +1,6 @@
 // phase_field.cpp — the APT driver (see phase_field.h).
 #include "phase_field.h"
+#include "../../include/cupf_host.h"
 
 #include <getopt.h>
 
@@ -255,8 +256,15 @@ bool PhaseField::parseInputImpl(const std::string& fileName) {
   mac.theta_arr.assign(nth, 0.f);
   mac.cost.assign(nth, 0.f);
   mac.sint.assign(nth, 0.f);
-  if (read_input(d + "/theta.txt", mac.theta_arr.data(), nth) < nth)
-    return setErr("theta.txt must hold 2*NG+1 angles");
+  if (read_input(d + "/theta.txt", mac.theta_arr.data(), nth) < nth) {
+    // no two-angle file: orientations as unit quaternions (w, x, y, z per grain)
+    std::vector<float> qf(4 * (size_t)p.num_theta);
+    if (read_input(d + "/quaternions.txt", qf.data(), (int)qf.size()) < (int)qf.size())
+      return setErr("theta.txt must hold 2*NG+1 angles (or quaternions.txt 4*NG values)");
+    std::vector<double> q(qf.begin(), qf.end());
+    if (cupf_host_quaternions_to_angles(p.num_theta, q.data(), mac.theta_arr.data()) != 0)
+      return setErr("quaternions.txt holds a zero or non-finite quaternion");
+  }
   // Temp.h5:/Temp (the 4-D temperature table, read only by nucleation): read from
   // Temp.txt (one value per line) when present, else zeros.
   read_input(d + "/Temp.txt", mac.T_3D.data(), (int)mac.T_3D.size());

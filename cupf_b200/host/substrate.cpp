@@ -18,6 +18,13 @@
 // Random numbers come from splitmix64 (a published 64-bit mixing generator),
 // uniform doubles from its top 53 bits, normals by the Box-Muller transform.
 // Points and angles use two streams of the same seed.
+//
+// Orientations given as unit quaternions map to the same two angles: the
+// kernel's rotation (APTPhaseField.cu:41-46) sends the lab direction with
+// azimuth theta_x and polar angle theta_z to the crystal z axis, so a grain's
+// angles are those of its crystal [001] axis in the lab frame, the third column
+// of the quaternion's rotation matrix.  The rotation about that axis, which the
+// two-angle model has no parameter for, is dropped.
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -79,6 +86,29 @@ extern "C" int cupf_host_voronoi_substrate(int nxp, int nyp, int num_grains, uin
     const double a = std::sqrt(-2.0 * std::log(u1)), b = std::sqrt(-2.0 * std::log(u3));
     const double ux = a * std::cos(2.0 * kPi * u2), uy = a * std::sin(2.0 * kPi * u2);
     const double uz = b * std::cos(2.0 * kPi * u4);
+    double tx = std::fmod(std::atan2(uy, ux), kPi);
+    if (tx < 0) tx += kPi;
+    const double tz = std::fmod(std::atan2(std::sqrt(ux * ux + uy * uy), uz), kPi);
+    theta[1 + g] = (float)tx;
+    theta[1 + num_grains + g] = (float)tz;
+  }
+  return 0;
+}
+
+extern "C" int cupf_host_quaternions_to_angles(int num_grains, const double* q, float* theta) {
+  if (num_grains < 1 || !q || !theta) return -1;
+  theta[0] = 0.0f;
+  for (int g = 0; g < num_grains; ++g) {
+    double w = q[4 * g], x = q[4 * g + 1], y = q[4 * g + 2], z = q[4 * g + 3];
+    const double nrm = std::sqrt(w * w + x * x + y * y + z * z);
+    if (!(nrm > 0.0) || !std::isfinite(nrm)) return -1;
+    w /= nrm;
+    x /= nrm;
+    y /= nrm;
+    z /= nrm;
+    // crystal [001] in the lab frame: R(q) (0, 0, 1)
+    const double ux = 2.0 * (x * z + w * y), uy = 2.0 * (y * z - w * x);
+    const double uz = 1.0 - 2.0 * (x * x + y * y);
     double tx = std::fmod(std::atan2(uy, ux), kPi);
     if (tx < 0) tx += kPi;
     const double tz = std::fmod(std::atan2(std::sqrt(ux * ux + uy * uy), uz), kPi);

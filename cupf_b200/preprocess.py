@@ -55,9 +55,24 @@ def native_substrate(nxp, nyp, num_grains, seed, periodic=True):
     return alpha, theta
 
 
+def quaternion_angles(q):
+    """Unit quaternions (w, x, y, z) per grain, shape (NG, 4), in the reference's
+    two-angle form [0, theta_x[1..NG], theta_z[1..NG]] (float32): the angles of
+    each grain's crystal [001] axis (cupf_host_quaternions_to_angles; the rotation
+    about that axis is dropped)."""
+    from . import abi
+    import ctypes as C
+    q = np.ascontiguousarray(q, np.float64).reshape(-1, 4)
+    theta = np.zeros(2 * len(q) + 1, np.float32)
+    if abi.lib().cupf_host_quaternions_to_angles(len(q), q.ctypes.data_as(C.POINTER(C.c_double)),
+                                                 theta.ctypes.data_as(C.POINTER(C.c_float))) != 0:
+        raise ValueError("zero or non-finite quaternion")
+    return theta
+
+
 def write_line_forcing(folder, Lx, Ly, Lz, num_grains, seed, G, R, z0, top, t_end,
                        periodic=True, macro=(13, 13, 23, 11), dxd=0.08, nmax=0.01,
-                       cooling_rate=None, substrate="cases"):
+                       cooling_rate=None, substrate="cases", quaternions=None):
     """The forcing folder of a line run: macro grid, psi = z0 - z, substrate ids
     (alpha.txt, (nx+1)x(ny+1) values), orientations, scalars.  nmax is the
     nucleation density (Nmax.txt).  With cooling_rate (K/s) the folder also holds
@@ -67,7 +82,9 @@ def write_line_forcing(folder, Lx, Ly, Lz, num_grains, seed, G, R, z0, top, t_en
 
     substrate: "cases" (the numpy generator the in-memory test cases use),
     "native" (the library's C++ generator), or an (alpha, theta) pair made
-    elsewhere, e.g. by the reference's own graph() (alpha (ny+1, nx+1))."""
+    elsewhere, e.g. by the reference's own graph() (alpha (ny+1, nx+1)).
+    quaternions: orientations as unit quaternions (NG, 4) written to
+    quaternions.txt in place of theta.txt (the drivers convert them)."""
     os.makedirs(folder, exist_ok=True)
     nxm, nym, nzm, ntm = macro
     BC = Lx / (nxm - 3)
@@ -100,7 +117,10 @@ def write_line_forcing(folder, Lx, Ly, Lz, num_grains, seed, G, R, z0, top, t_en
     put("t.txt", t)
     put("psi.txt", psi)
     put("alpha.txt", alpha.reshape(-1), "%d")
-    put("theta.txt", theta)
+    if quaternions is None:
+        put("theta.txt", theta)
+    else:
+        put("quaternions.txt", np.asarray(quaternions, np.float64).reshape(-1), "%1.8e")
     put("G.txt", [G])
     put("Rmax.txt", [R])
     put("V.txt", [0.0])

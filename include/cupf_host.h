@@ -68,6 +68,16 @@ int cupf_host_line_junctions_cells(int fnx, int fny, int nts, int num_nodes, con
 int cupf_host_voronoi_substrate(int nxp, int nyp, int num_grains, uint64_t seed, int periodic,
                                 int32_t* alpha, float* theta);
 
+/* Grain orientations given as unit quaternions (w, x, y, z per grain, normalised
+ * here) in the reference's two-angle form: theta (2*num_grains+1) gets
+ * [0, theta_x[1..NG], theta_z[1..NG]], the azimuth and polar angle (mod pi, as
+ * graph_datastruct.py:256-269) of each grain's crystal [001] axis in the lab
+ * frame, which the step's rotation (APTPhaseField.cu:41-46) sends to the crystal
+ * z axis.  The rotation about that axis has no parameter in the two-angle model
+ * and is dropped.  Returns 0, or -1 on a bad argument or a zero quaternion.
+ * The drivers read quaternions.txt (4*NG values) when theta.txt is absent. */
+int cupf_host_quaternions_to_angles(int num_grains, const double* q, float* theta);
+
 /* Writes alpha.txt ("%d" per line), theta.txt ("%1.4e" per line) and NG.txt
  * into an existing folder, as the reference's input scripts save them
  * (input_file.py:148-152).  Returns 0, or -1 on a bad argument or write. */

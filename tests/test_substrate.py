@@ -5,6 +5,9 @@
   nearest point with minimum-image distances, the reference's angle formula
   from graph_datastruct.py:256-269): identical ids, angles to float rounding.
 * Its files (cupf_host_write_substrate) in the reference's savetxt formats.
+* Orientations given as unit quaternions map to the reference's two angles
+  (those of the crystal [001] axis; the rotation about it is dropped), and the
+  driver reads quaternions.txt where theta.txt is absent.
 * Substrates made by the reference's own graph() (fixtures from
   tests/golden/substrate/make_graph_substrate.py) and by the library's generator
   load through the driver's forcing-folder reader exactly as through the
@@ -158,3 +161,67 @@ def test_native_substrate_loads_like_reference(built, tmp_path, monkeypatch):
         pytest.skip("reference host code not built: %s" % e)
     mine, theirs = _setup_both(tmp_path, monkeypatch, "native", 23, 11, 2.48)
     _assert_same(mine, theirs)
+
+
+# ---- orientations as unit quaternions ----
+
+def quat_mul(a, b):
+    w1, x1, y1, z1 = a
+    w2, x2, y2, z2 = b
+    return np.array([w1 * w2 - x1 * x2 - y1 * y2 - z1 * z2, w1 * x2 + x1 * w2 + y1 * z2 - z1 * y2,
+                     w1 * y2 - x1 * z2 + y1 * w2 + z1 * x2, w1 * z2 + x1 * y2 - y1 * x2 + z1 * w2])
+
+
+def quat_z_to(u):
+    """A unit quaternion rotating the z axis onto the unit vector u (shortest arc)."""
+    u = np.asarray(u, np.float64) / np.linalg.norm(u)
+    ax = np.cross([0.0, 0.0, 1.0], u)
+    s = np.linalg.norm(ax)
+    ang = math.atan2(s, u[2])
+    if s < 1e-15:
+        ax = np.array([1.0, 0.0, 0.0])
+    else:
+        ax = ax / s
+    return np.concatenate([[math.cos(ang / 2)], math.sin(ang / 2) * ax])
+
+
+def reference_angles(u):
+    """graph_datastruct.py:256-269 for one direction u."""
+    return math.atan2(u[1], u[0]) % math.pi, math.atan2(math.hypot(u[0], u[1]), u[2]) % math.pi
+
+
+def test_quaternions_map_to_the_reference_angles(built):
+    rng = np.random.default_rng(5)
+    us = rng.standard_normal((60, 3))
+    us /= np.linalg.norm(us, axis=1)[:, None]
+    q = np.stack([quat_z_to(u) for u in us])
+    q[::7] *= -2.5  # scale and sign do not matter
+    theta = preprocess.quaternion_angles(q)
+    want = np.array([reference_angles(u) for u in us])
+    assert theta[0] == 0
+    assert np.allclose(theta[1:61], want[:, 0], atol=2e-6) and np.allclose(theta[61:], want[:, 1], atol=2e-6)
+    # the rotation about the crystal [001] axis is the dropped third angle
+    spun = np.stack([quat_mul(qq, [math.cos(g / 2), 0.0, 0.0, math.sin(g / 2)])
+                     for qq, g in zip(q, rng.uniform(0, 2 * math.pi, 60))])
+    assert np.allclose(preprocess.quaternion_angles(spun), theta, atol=2e-6)
+    with pytest.raises(ValueError):
+        preprocess.quaternion_angles(np.zeros((2, 4)))
+
+
+def test_driver_reads_quaternions_in_place_of_angles(built, tmp_path, monkeypatch):
+    ng = 9
+    rng = np.random.default_rng(2)
+    us = rng.standard_normal((ng, 3))
+    q = np.stack([quat_z_to(u) for u in us])
+    folder = tmp_path / "forcing" / "case3"
+    preprocess.write_line_forcing(str(folder), 2.48, 2.48, 4.96, num_grains=ng, seed=3, G=1.0,
+                                  R=0.05, z0=0.6, top=0.3, t_end=5e-7, quaternions=q)
+    assert not (folder / "theta.txt").exists()
+    preprocess.write_input_file(str(tmp_path / "line.py"), 2.48, nts=2, asp_ratio_zx=2.0, num_pf=5)
+    monkeypatch.chdir(tmp_path)
+    st = host_api.setup_state("line.py", str(folder), bc=(1, 1, 0), line_config=True, cap=1 << 20)
+    # the file holds the quaternions to 9 digits; the driver converts them itself
+    qf = np.loadtxt(folder / "quaternions.txt").reshape(-1, 4).astype(np.float32).astype(np.float64)
+    theta = preprocess.quaternion_angles(qf)
+    assert np.allclose(st["sint"][:2 * ng + 1], np.sin(theta), atol=1e-6)
+    assert np.allclose(st["cost"][:2 * ng + 1], np.cos(theta), atol=1e-6)
