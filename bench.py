@@ -852,11 +852,13 @@ def run_apt3d(args, ws, rank, local):
         solver.set_skip_quiet(skip_quiet)
         solver.step(args.warmup)
         barrier()
-        solver.active_cells()  # restart the counter of computed cells
+        solver.active_cells()  # restart the counters of computed cells and merge overflows
+        solver.merge_overflows()
         clk = ClockSampler(device) if clocks else None
         if clk:
             clk.__enter__()
         ms = solver.time_steps(args.steps)
+        ovf = solver.merge_overflows()
         if clk:
             # keep the GPU under the same load for about half a second more, so the
             # sampler (100 ms period) sees the clocks of this kernel even when the
@@ -869,11 +871,14 @@ def run_apt3d(args, ws, rank, local):
         barrier()
         active = solver.active_cells() / args.steps  # cells of the computed items per launch
         ms = max_over_ranks(pg, ms, "cuda")
+        window.overflows = {"aliased_per_step": ovf[0] / args.steps,
+                            "dropped_per_step": ovf[1] / args.steps}
         return ms, active, clk.summary() if clk else None
 
     bytes_per_cell = {"fp32": 16, "fp16": 8, "bf16": 8}
     with APTSolver(case, precision=args.precision, device=device) as solver:
         ms, active, clocks = window(solver, False, clocks=True)
+        overflows = window.overflows
         ms_q, active_q, _ = window(solver, True)
     value = replica_throughput(ws, cells, args.steps, ms)
     bpc = NUM_PF * bytes_per_cell[args.precision]
@@ -977,7 +982,7 @@ def run_apt3d(args, ws, rank, local):
                                            "storage": args.precision}),
                 "hbm_gbs": achieved, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "quiet_skip": quiet, "precisions": precisions, "served": served,
-                "reference_kernels": ref_k,
+                "reference_kernels": ref_k, "merge_overflows": overflows,
                 "clocks": clocks, "gpu_launches": args.steps,
                 "baseline_metric": "3D APT Mcell-upd/s & HBM GB/s, mixed vs FP32; served sims/hr,"
                                    " p50/p99 at <=1e-3 err"}

@@ -118,6 +118,7 @@ def lib():
             "cupf_apt_set_wait_limit": [vp, C.c_int64],
             "cupf_apt_set_tile": [vp, C.c_int32],
             "cupf_apt_active_cells": [vp, C.POINTER(C.c_uint64)],
+            "cupf_apt_merge_overflows": [vp, C.POINTER(C.c_uint64)],
             "cupf_apt_nucl_init": [vp],
             "cupf_apt_nucleate": [vp, C.c_int32, C.POINTER(C.c_int32)],
             "cupf_apt_nucl_reset": [vp],

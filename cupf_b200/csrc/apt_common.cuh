@@ -69,6 +69,10 @@ struct StepArgs {
   const uint8_t* quiet_in;
   uint8_t* quiet_out;
   unsigned long long* active_cells;  // cells of the computed items, accumulated (may be NULL)
+  // merge overflows (more than NUM_PF distinct ids in a stencil), accumulated
+  // (may be NULL): [0] entries aliased into the next point's slot 0 (s < 6),
+  // [1] entries dropped at the last point (s == 6)
+  unsigned long long* overflows;
   long long wait_limit;  // SM cycles a stage wait may spin before the step gives up
 };
 

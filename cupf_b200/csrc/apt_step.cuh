@@ -270,6 +270,10 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
   // slot, or one whose id was just dropped: it keeps its last phi) or left one
   // unwritten; bits 1 and 2: the same in the item's bottom and top plane
   uint32_t live = 0;
+  // merge overflows of this thread's cells (StepArgs::overflows), aliased ones
+  // in the low 16 bits and dropped ones in the high 16 (at most 7 NP per cell
+  // and plane), summed per warp at the end of the item
+  uint32_t n_ovf = 0;
 
   const int gx = x0 + tx, gy = y0 + ty;
   const bool valid = gx <= a.fnx - 2 && gy <= a.fny - 2;
@@ -376,6 +380,7 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
               code[s + 1] = nib_insert(code[s + 1], 0xEu, 0);
               alias[s + 1] = S::phi(pr);
             }
+            n_ovf += s < 6 ? 1u : 0x10000u;
             continue;
           }
         }
@@ -550,6 +555,14 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
   if (tid == 0 && a.quiet_out)
     a.quiet_out[(zci * a.nty + tyi) * a.ntx + txi] =
         (uint8_t)((busy ? 0 : 1) | (busy_lo ? 0 : 2) | (busy_hi ? 0 : 4));
+  if (a.overflows) {
+    const uint32_t wa = __reduce_add_sync(0xffffffffu, n_ovf & 0xFFFFu);
+    const uint32_t wd = __reduce_add_sync(0xffffffffu, n_ovf >> 16);
+    if ((tid & 31) == 0 && (wa | wd)) {
+      atomicAdd(a.overflows, (unsigned long long)wa);
+      atomicAdd(a.overflows + 1, (unsigned long long)wd);
+    }
+  }
   if (tid == 0 && a.active_cells) {
     const int wx = min(TX, a.fnx - 1 - x0), wy = min(TY, a.fny - 1 - y0);
     atomicAdd(a.active_cells, (unsigned long long)(wx * wy * (k_end - k_begin)));

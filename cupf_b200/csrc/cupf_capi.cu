@@ -101,6 +101,7 @@ struct cupf_apt_handle {
   long long wait_limit = kWaitCycles;  // stage-wait bound of the step kernel (SM cycles)
   bool zc_user = false;  // z chunk fixed by the caller (set_tuning or CUPF_ZC)
   unsigned long long* active_cells = nullptr;
+  unsigned long long* overflows = nullptr;  // merge overflows: [0] aliased, [1] dropped
   // read-back scratch (reference layout, num_pf * length), allocated on first use
   float* xfer_ph = nullptr;
   int* xfer_id = nullptr;
@@ -200,7 +201,7 @@ static void free_handle(cupf_apt_handle* h) {
                   h->xfer_ph, h->xfer_id, h->layer_sums, h->alpha_full, h->loss_area,
                   h->counts, h->first, h->qoi_part, h->nucl_status, h->nucl_count,
                   h->nucl_sphere, h->jcand, h->jcount, h->jdistinct, h->quiet[0], h->quiet[1],
-                  h->active_cells, h->z64};
+                  h->active_cells, h->overflows, h->z64};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -519,6 +520,8 @@ extern "C" cupf_status cupf_apt_create(const cupf_apt_params* p, const cupf_apt_
   }
   TRY(cuda(cudaMalloc((void**)&h->active_cells, sizeof(unsigned long long)), "counter"));
   TRY(cuda(cudaMemsetAsync(h->active_cells, 0, sizeof(unsigned long long), h->stream), "memset"));
+  TRY(cuda(cudaMalloc((void**)&h->overflows, 2 * sizeof(unsigned long long)), "counter"));
+  TRY(cuda(cudaMemsetAsync(h->overflows, 0, 2 * sizeof(unsigned long long), h->stream), "memset"));
   TRY(cuda(cudaMalloc((void**)&h->layer_sums, p->fnz * sizeof(double)), "layer sums"));
   for (int b = 0; b < 2; ++b) TRY(make_tmap(h, b));
   const char* zc_env = getenv("CUPF_ZC");
@@ -574,6 +577,18 @@ extern "C" cupf_status cupf_apt_set_skip_quiet(cupf_apt_handle* h, int32_t enabl
   CK(cudaSetDevice(h->device));
   h->skip_quiet = enable != 0;
   return invalidate_quiet(h);
+}
+
+extern "C" cupf_status cupf_apt_merge_overflows(cupf_apt_handle* h, uint64_t* counts) {
+  if (!h || !counts) return fail(CUPF_ERR_INVALID, "null argument");
+  CK(cudaSetDevice(h->device));
+  unsigned long long v[2] = {0, 0};
+  CK(cudaMemcpyAsync(v, h->overflows, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemsetAsync(h->overflows, 0, sizeof(v), h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  counts[0] = v[0];
+  counts[1] = v[1];
+  return CUPF_OK;
 }
 
 extern "C" cupf_status cupf_apt_active_cells(cupf_apt_handle* h, uint64_t* cells) {
@@ -721,6 +736,7 @@ extern "C" cupf_status cupf_apt_step(cupf_apt_handle* h, int32_t nsteps,
       a.quiet_out = h->quiet[h->cur ^ 1];
     }
     a.active_cells = h->active_cells;
+    a.overflows = h->overflows;
     cupf_status st = launch_step(h, a, h->tmap[h->cur]);
     if (st) return st;
     h->cur ^= 1;

@@ -170,6 +170,12 @@ class APTSolver:
         """Leave work items whose cells stay all-empty alone (default on)."""
         abi.check(self.L.cupf_apt_set_skip_quiet(self.h, int(bool(enable))))
 
+    def merge_overflows(self):
+        """(aliased, dropped) merge-overflow entries since the last call."""
+        v = (C.c_uint64 * 2)()
+        abi.check(self.L.cupf_apt_merge_overflows(self.h, v))
+        return int(v[0]), int(v[1])
+
     def active_cells(self):
         """Cells of the computed (not quiet) work items since the last call."""
         v = C.c_uint64()

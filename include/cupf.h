@@ -336,6 +336,13 @@ cupf_status cupf_apt_set_skip_quiet(cupf_apt_handle* h, int32_t enable);
  * that path. */
 cupf_status cupf_apt_set_wait_limit(cupf_apt_handle* h, int64_t cycles);
 
+/* Merge overflows since the last call (hazard H1 of the reference's merge,
+ * APTPhaseField.cu:222-231: a stencil holding more than NUM_PF distinct ids):
+ * counts[0] = entries written to local_phs[s][NUM_PF], which aliases the next
+ * point's slot 0 (s < 6, reproduced), counts[1] = entries past the array at the
+ * last point (s == 6, dropped).  Resets both. */
+cupf_status cupf_apt_merge_overflows(cupf_apt_handle* h, uint64_t* counts);
+
 /* Cells of the work items the step computed (not left alone as quiet) since the
  * previous call, summed over steps; the counter restarts at 0. */
 cupf_status cupf_apt_active_cells(cupf_apt_handle* h, uint64_t* cells);

@@ -33,8 +33,8 @@
  * Semantics pinned explicitly where the reference is undefined:
  *   H1 merge overflow (more than NUM_PF distinct ids in a 7-point stencil): the
  *      reference writes local_phs[s][NUM_PF], which aliases local_phs[s+1][0]
- *      for s < 6 (restated here), and lands past the array for s == 6 (dropped
- *      here; counted in stats[1]).
+ *      for s < 6 (restated here; entries counted in stats[0]), and lands past
+ *      the array for s == 6 (dropped here; counted in stats[1]).
  *   Boundary edges/corners: APTsetBC3D fills faces in parallel, so cells on two
  *      or three halo faces race in the reference.  Here every halo coordinate is
  *      mapped independently, which is what sequential z, y, x face fills give.
@@ -126,7 +126,7 @@ static inline grid_t mkgrid(const cupf_apt_params* p) {
  * stencil points (D,B,L,C,R,T,U) x slots, exactly as APTPhaseField.cu:211-233,
  * and src[s][j] = flat index whose phi feeds local_phs[s][j] (-1 -> -1.0). */
 static inline void apt_merge(const grid_t* g, int64_t C, const int32_t* aarg, int32_t* L,
-                             int64_t src[7][NPMAX], int64_t* n_overflow_u) {
+                             int64_t src[7][NPMAX], int64_t* n_overflow_u, int64_t* n_alias) {
   const int np = g->np;
   for (int a = 0; a < np; ++a) {
     L[a] = -1;
@@ -151,6 +151,7 @@ static inline void apt_merge(const grid_t* g, int64_t C, const int32_t* aarg, in
         src[s][a] = gc;
       } else if (s < 6) {
         src[s + 1][0] = gc; /* local_phs[s][NUM_PF] == local_phs[s+1][0] */
+        (*n_alias)++;
       } else {
         (*n_overflow_u)++;
       }
@@ -270,21 +271,21 @@ static int tinterp_f32(const cupf_apt_params* p, const cupf_apt_inputs* th, int 
 }
 
 /* One explicit step, single precision.  stats (may be NULL): [0] cells with a
- * merge overflow at s<6 (aliased), [1] entries dropped at s==6. */
+ * merge overflow entries at s<6 (aliased), [1] entries dropped at s==6. */
 void oracle_rhs_psi_f32(const cupf_apt_params* p, const cupf_apt_inputs* th, float t,
                         const float* ph, float* ph_new, const int32_t* aarg, int32_t* aarg_new,
                         int use_iuc, int64_t* stats) {
   grid_t g = mkgrid(p);
   const int np = g.np;
-  int64_t ovf_u = 0;
-#pragma omp parallel for collapse(2) schedule(static) reduction(+ : ovf_u)
+  int64_t ovf_u = 0, ovf_a = 0;
+#pragma omp parallel for collapse(2) schedule(static) reduction(+ : ovf_u, ovf_a)
   for (int j = 1; j < g.fny - 1; ++j) {
     for (int i = 1; i < g.fnx - 1; ++i) {
       for (int k = 1; k < g.fnz - 1; ++k) {
         int64_t C = (int64_t)k * g.fnx * g.fny + (int64_t)j * g.fnx + i;
         int32_t L[NPMAX];
         int64_t src[7][NPMAX];
-        apt_merge(&g, C, aarg, L, src, &ovf_u);
+        apt_merge(&g, C, aarg, L, src, &ovf_u, &ovf_a);
         float lp[7][NPMAX];
         for (int s = 0; s < 7; ++s)
           for (int a = 0; a < np; ++a) lp[s][a] = src[s][a] >= 0 ? ph[src[s][a]] : -1.0f;
@@ -342,7 +343,10 @@ void oracle_rhs_psi_f32(const cupf_apt_params* p, const cupf_apt_inputs* th, flo
       }
     }
   }
-  if (stats) stats[1] += ovf_u;
+  if (stats) {
+    stats[0] += ovf_a;
+    stats[1] += ovf_u;
+  }
 }
 
 /* ---------------------------------------------------------------- FP64 mode */
@@ -375,15 +379,15 @@ int oracle_rhs_psi_f64(const cupf_apt_params* p, const oracle_thermal_f64* th, d
   if (!use_iuc && p->thermalType != 0 && p->thermalType != 1 && p->thermalType != 5) return -1;
   grid_t g = mkgrid(p);
   const int np = g.np;
-  int64_t ovf_u = 0;
-#pragma omp parallel for collapse(2) schedule(static) reduction(+ : ovf_u)
+  int64_t ovf_u = 0, ovf_a = 0;
+#pragma omp parallel for collapse(2) schedule(static) reduction(+ : ovf_u, ovf_a)
   for (int j = 1; j < g.fny - 1; ++j) {
     for (int i = 1; i < g.fnx - 1; ++i) {
       for (int k = 1; k < g.fnz - 1; ++k) {
         int64_t C = (int64_t)k * g.fnx * g.fny + (int64_t)j * g.fnx + i;
         int32_t L[NPMAX];
         int64_t src[7][NPMAX];
-        apt_merge(&g, C, aarg, L, src, &ovf_u);
+        apt_merge(&g, C, aarg, L, src, &ovf_u, &ovf_a);
         double lp[7][NPMAX];
         for (int s = 0; s < 7; ++s)
           for (int a = 0; a < np; ++a) lp[s][a] = src[s][a] >= 0 ? ph[src[s][a]] : -1.0;
@@ -439,7 +443,10 @@ int oracle_rhs_psi_f64(const cupf_apt_params* p, const oracle_thermal_f64* th, d
       }
     }
   }
-  if (stats) stats[1] += ovf_u;
+  if (stats) {
+    stats[0] += ovf_a;
+    stats[1] += ovf_u;
+  }
   return 0;
 }
 
