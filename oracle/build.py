@@ -42,17 +42,16 @@ from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
+# Where this recipe finds the reference's sources when CUPF_REFERENCE_ROOT does not
+# name them (the reference is read in place, never copied into the repository).
+DEFAULT_REFERENCE_ROOT = "/root/reference"
+
+
 def _reference_root():
-    """The reference tree: CUPF_REFERENCE_ROOT, else the reference_path recorded
-    in the repository's BASELINE.json (None when neither names a directory)."""
-    root = os.environ.get("CUPF_REFERENCE_ROOT")
-    if not root:
-        try:
-            import json
-            root = json.load(open(os.path.join(ROOT, "BASELINE.json"))).get("reference_path")
-        except Exception:
-            root = None
-    return root if root and os.path.isdir(root) else None
+    """The reference tree: CUPF_REFERENCE_ROOT, else DEFAULT_REFERENCE_ROOT (None
+    when neither is a directory, as on a machine without the reference)."""
+    root = os.environ.get("CUPF_REFERENCE_ROOT") or DEFAULT_REFERENCE_ROOT
+    return root if os.path.isdir(root) else None
 
 
 _REF_ROOT = _reference_root()
