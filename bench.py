@@ -373,8 +373,12 @@ def serve_stream(prec, nreq, fix=None, device=0):
             "arrival_rate_per_s": 4.0, "steps_per_request": SERVE_STEPS,
             "capacity": {"sims_per_hr": len(sat) / sat_span * 3600.0,
                          "mcell_upd_per_s": cells / sat_span / 1e6, "seconds": sat_span,
-                         "device_busy_s": busy, "clocks": clk_sat.summary(),
-                         "note": "the same requests all submitted at once"},
+                         "device_busy_s": busy,
+                         "device_mcell_upd_per_s": cells / busy / 1e6 if busy > 0 else None,
+                         "clocks": clk_sat.summary(),
+                         "note": "the same requests all submitted at once; the device rate "
+                                 "counts the rounds' device time only (the span also holds "
+                                 "admission, retirement and host time)"},
             "errors_vs_fp64": {"results": errors, "worst": worst, "tolerance": ERROR_TOL,
                                "which": "every 48^3 request of the stream (the oracle's cost "
                                         "bounds the rest)"},
