@@ -9,9 +9,9 @@
 // the initial psi/U from the 1-D profiles, runs the psi-only pre-step and Mt
 // fused steps (with the tip search and moving frame every TIPP steps), and
 // writes phi, the concentration c/c_inf and the coordinates (y - ztip0) as
-// line_nx<nx>_ny<ny>_Mt<Mt>_seed<seed>.npz (the reference writes the same
-// datasets to an .h5 file; HDF5 is not available to this build), plus the tip
-// height and primary spacing.
+// line_nx<nx>_ny<ny>_Mt<Mt>_seed<seed>.h5, the reference's datasets, through the
+// library's HDF5 writer (.npz when CUPF_OUTPUT_FORMAT=npz), plus the tip height
+// and primary spacing.
 //
 // Input keys beyond the reference's: perturb_sites / perturb_amp add the seeded
 // front perturbation of cupf_host_ek2d_perturb; cfl defaults to 0.8 when absent
