@@ -54,13 +54,18 @@ FP64_QOI = os.path.join(ROOT, "tests", "golden", "fp64", "qoi.npz")
 ERROR_TOL = 1e-3  # relative error bound on volume fractions and interface position
 
 
-def workload_config(extra=None):
+def workload_config(extra=None, pair_bytes=8):
+    """The workload's description; `pair_bytes` is the size of one stored
+    (phi, id) slot (8 for FP32 storage, 4 for the 16-bit forms)."""
+    nx, ny, nz = INTERIOR
+    buf = (nx + 2) * (ny + 2) * (nz + 2) * NUM_PF * pair_bytes
     c = {"workload": "3D APT line step %dx%dx%d interior, NUM_PF=%d, %d grains"
                      % (*INTERIOR, NUM_PF, GRAINS),
          "interior": list(INTERIOR), "num_pf": NUM_PF, "grains": GRAINS, "seed": SEED,
          "bc": "110", "thermal": "line G=1 K/um R=0.05 m/s", "config_steps": CONFIG_STEPS,
          "sweep": "every work item computed",
-         "l2": "inputs larger than L2 (2 x 2.2 GB pair buffers), no flush"}
+         "l2": "inputs %s L2 (2 x %.1f MB pair buffers against 126 MB), no flush"
+               % ("larger than" if buf > 126e6 else "NOT larger than", buf / 1e6)}
     if extra:
         c.update(extra)
     return c
@@ -983,7 +988,8 @@ def run_apt3d(args, ws, rank, local):
                 "dtype": "fp32" if args.precision == "fp32" else args.precision + " storage, fp32 compute",
                 "data": "synthetic",
                 "config": workload_config({"parallelism": "replicas x%d" % ws,
-                                           "storage": args.precision}),
+                                           "storage": args.precision},
+                                          8 if args.precision == "fp32" else 4),
                 "hbm_gbs": achieved, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "quiet_skip": quiet, "precisions": precisions, "served": served,
                 "reference_kernels": ref_k, "merge_overflows": overflows,
