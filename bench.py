@@ -20,7 +20,7 @@ The same line also carries, on one GPU: the FP16- and BF16-storage steps on the
 same workload ("mixed vs FP32"), the errors of FP32/FP16/BF16 storage against
 the FP64 oracle (64^3 case, 1000 steps, fixture tests/golden/fp64/qoi.npz), the
 served stream (sims/hr, p50/p99 time-to-result, capacity, per-result errors of
-the 48^3 requests against FP64-oracle fixtures), the reference's own
+the 48^3 and 96^3 requests against FP64-oracle fixtures), the reference's own
 APTsetBC3D + APTrhs_psi kernels compiled for sm_100a timed on the same state,
 and the host-CPU baseline.
 
@@ -293,8 +293,8 @@ def serve_stream(prec, nreq, fix=None, device=0):
     """Continuous-batching run of the seeded Poisson stream: submit each request
     at its arrival time, pump the server meanwhile; then the same requests all
     submitted at once (capacity).  Returns sims/hr, p50/p99 time-to-result,
-    cell-update rates and, for the 48^3 requests, each result's error against
-    the FP64 oracle (fixture)."""
+    cell-update rates and, for the requests the FP64-oracle fixture covers
+    (the 48^3 and 96^3 grids), each result's error against it."""
     from cupf_b200.server import SERVE_GRIDS, Server, poisson_stream
     reqs = poisson_stream(nreq, seed=0, num_pf=NUM_PF)
     fix_idx = set(int(i) for i in fix["served_index"]) if fix is not None else set()
@@ -385,8 +385,11 @@ def serve_stream(prec, nreq, fix=None, device=0):
                                  "counts the rounds' device time only (the span also holds "
                                  "admission, retirement and host time)"},
             "errors_vs_fp64": {"results": errors, "worst": worst, "tolerance": ERROR_TOL,
-                               "which": "every 48^3 request of the stream (the oracle's cost "
-                                        "bounds the rest)"},
+                               "which": "every request of the stream with a %s grid (%d of %d; "
+                                        "the oracle's cost bounds the rest)"
+                                        % (" or ".join(sorted({"x".join(map(str, e["grid"]))
+                                                               for e in errors})) or "no",
+                                           len(errors), len(res))},
             "clocks": clk.summary()}
 
 
