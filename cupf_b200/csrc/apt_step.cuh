@@ -56,8 +56,16 @@ struct StepSmem {
   static constexpr int kStageBytes = (kBoxBytes + 127) & ~127;  // stage stride (TMA dst: 128 B aligned)
   static constexpr int kStagePairs = kStageBytes / S::kBytes;
   static constexpr int kMaskOff = STAGES * kStageBytes;
-  static constexpr int kBarOff = (kMaskOff + STAGES * BCELLS * 2 + 7) & ~7;
-  static constexpr int kBytes = kBarOff + STAGES * 8 + 16;  // + abort word, issued count
+  // 16-bit pairs in 32x8 tiles: the centre plane's phi values decoded once per
+  // plane into FP32 (slot-major like a stage, plus one row of -1 that the absent
+  // code NP points at), read by the five stencil points in that plane.  Three
+  // CTAs per SM still fit; for 32x4 tiles the extra row would cost one.
+  static constexpr bool kDecode = S::kBytes == 4 && TY == 8;
+  static constexpr int kDecOff = (kMaskOff + STAGES * BCELLS * 2 + 15) & ~15;
+  static constexpr int kDecBytes = kDecode ? (NP + 1) * BCELLS * 4 : 0;
+  static constexpr int kBarOff = (kDecOff + kDecBytes + 7) & ~7;
+  // + abort word, issued count, item index, one occupancy flag per stage
+  static constexpr int kBytes = kBarOff + STAGES * 8 + 16 + STAGES * 4;
 };
 
 // Per-slot update loop shape of a storage format: rolled for the 16-bit pairs,
@@ -162,17 +170,21 @@ struct CtaSmem {
   using Smem = StepSmem<NP, S, TY>;
   P* stages;
   uint16_t* masks;
+  float* dec;     // decoded centre plane (Smem::kDecode)
   uint64_t* bars;
   int* s_abort;   // global plane sequence number of the first failed wait, + 1
   int* s_issued;  // plane sequence numbers issued so far (written by thread 0)
   int* s_item;    // work item handed to the CTA (batched kernel)
+  int* s_occ;     // per stage: some cell of the landed plane holds an id
   __device__ explicit CtaSmem(unsigned char* smem) {
     stages = reinterpret_cast<P*>(smem);
     masks = reinterpret_cast<uint16_t*>(smem + Smem::kMaskOff);
+    dec = reinterpret_cast<float*>(smem + Smem::kDecOff);
     bars = reinterpret_cast<uint64_t*>(smem + Smem::kBarOff);
     s_abort = reinterpret_cast<int*>(smem + Smem::kBarOff + STAGES * 8);
     s_issued = s_abort + 1;
     s_item = s_abort + 2;
+    s_occ = s_abort + 4;
   }
   __device__ void init() {
     if (threadIdx.x == 0) {
@@ -181,6 +193,8 @@ struct CtaSmem {
       *s_issued = 0;
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    if (Smem::kDecode)
+      for (int c = threadIdx.x; c < Smem::BCELLS; c += blockDim.x) dec[NP * Smem::BCELLS + c] = -1.0f;
     __syncthreads();
   }
   // After a timed-out wait no further loads are issued; before the CTA exits
@@ -210,6 +224,12 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
   using P = typename S::T;
   constexpr int BW = Smem::BW;
   constexpr int BCELLS = Smem::BCELLS;
+  constexpr bool kDec = Smem::kDecode;
+  // code of an absent source slot: NP (the decoded plane's row of -1) where the
+  // centre plane is decoded, else 0xF; 0xE marks the aliased overflow value
+  constexpr uint32_t kAbsent = kDec ? (uint32_t)NP : 0xFu;
+  // offsets of the centre plane's stencil points B, L, C, R, T from the cell
+  constexpr int ctr_off[7] = {0, -BW, -1, 0, 1, BW, 0};
   P* stages = sm.stages;
   uint16_t* masks = sm.masks;
   uint64_t* bars = sm.bars;
@@ -233,6 +253,7 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
     const int s = g % STAGES;
     const int zl = k_begin - 1 + q;
     const int zp = bc_map(zl, a.fnz, a.bcZ);
+    if (kDec) sm.s_occ[s] = 0;
     mbar_arrive_expect_tx(&bars[s], Smem::kBoxBytes);
     tma_load_plane(stages + (size_t)s * Smem::kStagePairs, tmap, &bars[s], x0 - 1, y0 - 1, zp);
     *s_issued = g + 1;
@@ -256,12 +277,15 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
       atomicExch(a.err, ERR_TMA_TIMEOUT);
     }
     const P* st = stages + (size_t)s * Smem::kStagePairs;
+    uint32_t any = 0;
     for (int c = tid; c < BCELLS; c += NTHREADS) {
       uint32_t m = 0;
 #pragma unroll
       for (int p = 0; p < NP; ++p) m |= (uint32_t)(S::id(st[p * BCELLS + c]) != -1) << p;
       masks[s * BCELLS + c] = (uint16_t)m;
+      any |= m;
     }
+    if (kDec && any) sm.s_occ[s] = 1;
   };
 
   land(0);
@@ -306,9 +330,17 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
       fence_proxy_async();
       issue(qk - 2 + STAGES);
     }
+    const int sD = (q0 + qk - 1) % STAGES, sC = (q0 + qk) % STAGES, sU = (q0 + qk + 1) % STAGES;
+    // decode the centre plane's phi once (a plane without ids needs none: every
+    // code into it is then absent); every thread has finished the previous
+    // plane, the last reader of the decoded values, at the barrier above
+    if (kDec && sm.s_occ[sC]) {
+      const P* st = stages + (size_t)sC * Smem::kStagePairs;
+      for (int e = tid; e < NP * BCELLS; e += NTHREADS) sm.dec[e] = S::phi(st[e]);
+      __syncthreads();
+    }
     if (!valid) continue;
 
-    const int sD = (q0 + qk - 1) % STAGES, sC = (q0 + qk) % STAGES, sU = (q0 + qk + 1) % STAGES;
     const P* pD = stages + (size_t)sD * Smem::kStagePairs + c;
     const P* pC = stages + (size_t)sC * Smem::kStagePairs + c;
     const P* pU = stages + (size_t)sU * Smem::kStagePairs + c;
@@ -352,9 +384,10 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
     float alias[7];
 #pragma unroll
     for (int s = 0; s < 7; ++s) {
-      code[s] = ~(Map)0;
+      code[s] = kDec ? (Map)(0x11111111u * kAbsent) : ~(Map)0;
       alias[s] = -1.0f;
     }
+    bool has_alias = false;  // some point's slot 0 holds an aliased overflow value
     // General visit of stencil point s: each occupied slot's id is looked up in
     // the list and appended when new (APTPhaseField.cu:211-233).
     auto merge_point = [&](int s) {
@@ -379,6 +412,7 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
             if (s < 6) {
               code[s + 1] = nib_insert(code[s + 1], 0xEu, 0);
               alias[s + 1] = S::phi(pr);
+              has_alias = true;
             }
             n_ovf += s < 6 ? 1u : 0x10000u;
             continue;
@@ -433,14 +467,25 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
     merge_point(5);
     if (!identity_point(6)) merge_point(6);
 
-    // Value of output slot j at stencil point s: 0xF = absent (-1), 0xE = the
-    // aliased overflow value, which only ever lands in slot 0.
-    auto fetch = [&](int s, int j) -> float {
+    // Value of output slot j at stencil point s: kAbsent = absent (-1), 0xE = the
+    // aliased overflow value, which only ever lands in slot 0 (kAlias false: the
+    // caller knows no point of the cell has one).  The five points of the centre
+    // plane read the decoded plane where there is one.
+    auto fetch = [&](int s, int j, auto alias_tag) -> float {
+      constexpr bool kAlias = decltype(alias_tag)::value;
       const uint32_t cd = (uint32_t)(code[s] >> (4 * j)) & 0xF;
-      if (j == 0 && cd == 0xE) return alias[s];
-      if (cd == 0xF) return -1.0f;
+      const bool al = kAlias && j == 0 && cd == 0xEu;
+      if (kDec && s >= 1 && s <= 5) {
+        // the index stays inside the decoded plane for the alias code too
+        const float v = sm.dec[(al ? kAbsent : cd) * BCELLS + c + ctr_off[s]];
+        return al ? alias[s] : v;
+      }
+      if (al) return alias[s];
+      if (cd == kAbsent) return -1.0f;
       return S::phi(pts[s][cd * BCELLS]);
     };
+    using WithAlias = std::integral_constant<bool, true>;
+    using NoAlias = std::integral_constant<bool, false>;
 
     // phi + 1 at the centre for every slot (the repulsion sum's terms); the loops
     // over slots stop at n, so a warp runs only as many iterations as its
@@ -451,7 +496,7 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
 #pragma unroll
     for (int q = 0; q < NP; ++q) {
       if (q >= n) break;
-      phc1[q] = __fadd_rn(fetch(3, q), 1.0f);
+      phc1[q] = __fadd_rn(fetch(3, q, WithAlias{}), 1.0f);
     }
 
     // rounding bits of this cell and step: keyed on the cell's reference-layout
@@ -469,7 +514,7 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
     }
 
     // New value of output slot j < n holding grain `id`.
-    auto update_slot = [&](int j, int id) -> P {
+    auto update_slot = [&](int j, int id, auto alias_tag) -> P {
       // orientation of the grain (APTPhaseField.cu:259-273): loads issued before
       // the stencil values are gathered so their latency overlaps; ids are >= 0
       // here (cupf_apt_set_slots rejects other negative ids) and the clamp only
@@ -482,7 +527,7 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
       const float4 t_o = __ldg(a.orient + ti);  // {sint[ti], cost[ti], sint[ti+NG], cost[ti+NG]}
       float ph7[7];
 #pragma unroll
-      for (int s = 0; s < 7; ++s) ph7[s] = fetch(s, j);
+      for (int s = 0; s < 7; ++s) ph7[s] = fetch(s, j, alias_tag);
       float sina = 0.0f, cosa = 1.0f, sinb = 0.0f, cosb = 1.0f;
       if (ph7[3] > kLS && tab_ok) {  // (double)phC > LS
         sina = t_o.x;
@@ -519,15 +564,23 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
       for (int j = 0; j < NP; ++j)
         if (j >= n) put(j, S::empty());
       if (upd) {
+        auto slots = [&](auto alias_tag) {
 #pragma unroll 1
-        for (int j = 0; j < n; ++j) {
-          int id = L[0];
+          for (int j = 0; j < n; ++j) {
+            int id = L[0];
 #pragma unroll
-          for (int q = 1; q < NP; ++q) id = (j == q) ? L[q] : id;
-          const P v = update_slot(j, id);
-          clive |= !S::is_empty(v);
-          put(j, v);
-        }
+            for (int q = 1; q < NP; ++q) id = (j == q) ? L[q] : id;
+            const P v = update_slot(j, id, alias_tag);
+            clive |= !S::is_empty(v);
+            put(j, v);
+          }
+        };
+        // merge overflows are rare: a warp none of whose cells has an aliased
+        // value runs the loop without the alias checks
+        if (__any_sync(__activemask(), has_alias))
+          slots(WithAlias{});
+        else
+          slots(NoAlias{});
       } else {
         clive = true;
       }
@@ -537,7 +590,7 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
         if (j >= n) {
           put(j, S::empty());
         } else if (upd) {
-          const P v = update_slot(j, L[j]);
+          const P v = update_slot(j, L[j], WithAlias{});
           clive |= !S::is_empty(v);
           put(j, v);
         } else {
