@@ -334,10 +334,19 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
     // decode the centre plane's phi once (a plane without ids needs none: every
     // code into it is then absent); every thread has finished the previous
     // plane, the last reader of the decoded values, at the barrier above
-    if (kDec && sm.s_occ[sC]) {
-      const P* st = stages + (size_t)sC * Smem::kStagePairs;
-      for (int e = tid; e < NP * BCELLS; e += NTHREADS) sm.dec[e] = S::phi(st[e]);
-      __syncthreads();
+    if constexpr (kDec) {
+      if (sm.s_occ[sC]) {
+        // four pairs per thread and pass (a stage and the decoded plane start on
+        // 16-byte boundaries; NP * BCELLS is a multiple of 4)
+        static_assert((NP * BCELLS) % 4 == 0, "vector decode");
+        const uint4* st = reinterpret_cast<const uint4*>(stages + (size_t)sC * Smem::kStagePairs);
+        float4* d4 = reinterpret_cast<float4*>(sm.dec);
+        for (int e = tid; e < NP * BCELLS / 4; e += NTHREADS) {
+          const uint4 w = st[e];
+          d4[e] = make_float4(S::phi(w.x), S::phi(w.y), S::phi(w.z), S::phi(w.w));
+        }
+        __syncthreads();
+      }
     }
     if (!valid) continue;
 
@@ -565,11 +574,18 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
         if (j >= n) put(j, S::empty());
       if (upd) {
         auto slots = [&](auto alias_tag) {
+          // the list's ids (16-bit in these formats) packed two to a word and
+          // shifted down one id per slot: slot j's id is always the low half
+          uint32_t w[(NP + 1) / 2];
+#pragma unroll
+          for (int q = 0; q < (NP + 1) / 2; ++q)
+            w[q] = __byte_perm((uint32_t)L[2 * q], 2 * q + 1 < NP ? (uint32_t)L[2 * q + 1] : 0u, 0x5410);
 #pragma unroll 1
           for (int j = 0; j < n; ++j) {
-            int id = L[0];
+            const int id = (int)(short)(w[0] & 0xFFFFu);
 #pragma unroll
-            for (int q = 1; q < NP; ++q) id = (j == q) ? L[q] : id;
+            for (int q = 0; q < (NP + 1) / 2 - 1; ++q) w[q] = __funnelshift_r(w[q], w[q + 1], 16);
+            w[(NP + 1) / 2 - 1] >>= 16;
             const P v = update_slot(j, id, alias_tag);
             clive |= !S::is_empty(v);
             put(j, v);
