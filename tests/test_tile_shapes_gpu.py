@@ -3,7 +3,8 @@ autotuner picks one per grid shape with the z chunk): results are identical
 bit for bit whichever tile shape steps a simulation.
 
 * single handle, 32x4 against 32x8: partial tiles in y, every boundary code,
-  FP32 and FP16, z chunks of 1 to 16, quiet items on;
+  FP32, FP16 and BF16 (the 16-bit 32x8 kernel decodes each centre plane once,
+  the 32x4 one per use), merge overflows, z chunks of 1 to 16, quiet items on;
 * 32x4 against the reference kernels on a parity case;
 * the server with every request on 32x4, on 32x8, and with the two mixed in one
   round (one batched launch per tile height), against the single handle.
@@ -25,6 +26,10 @@ CASES = [
     ((40, 42, 48), 8, 90, 7, "110", 60, 16, "fp32"),
     ((24, 26, 40), 8, 60, 1, "000", 30, 8, "fp16"),
     ((48, 44, 56), 8, 70, 3, "110", 80, 4, "bf16"),
+    # few slots, many grains: merge overflows, whose aliased values the 16-bit
+    # 32x8 kernel reads through its decoded centre plane and the 32x4 one per use
+    ((36, 30, 40), 3, 60, 3, "110", 25, 4, "fp16"),
+    ((48, 40, 32), 4, 120, 4, "011", 25, 2, "bf16"),
 ]
 
 
