@@ -112,6 +112,11 @@ struct cupf_server {
   double* d_part = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
+  // the requests' device memory: a stream-ordered pool that keeps what retired
+  // requests free for the next admissions (no release to the driver until the
+  // server is destroyed), so admitting and retiring cost no device-wide
+  // allocation or synchronising free
+  cudaMemPool_t pool = nullptr;
   bool dirty = true;
   // (fnx, fny, fnz) -> (tile height, z chunk)
   std::map<std::tuple<int, int, int>, std::pair<int, int>> tile_cache;
@@ -138,11 +143,18 @@ static int gridn(long long n) {
   return (int)std::max(1ll, std::min(b, 148ll * 16));
 }
 
-static void free_request_device(Request* r) {
+// A request's device buffer from the server's pool, ordered on its stream.
+static cudaError_t pool_alloc(cupf_server* s, void** p, size_t n) {
+  return cudaMallocFromPoolAsync(p, n, s->pool, s->stream);
+}
+
+// Return a request's buffers to the pool (ordered after the work queued on the
+// server's stream that reads them).
+static void free_request_device(cupf_server* s, Request* r) {
   void* ptrs[] = {r->buf[0], r->buf[1], r->dx, r->dy, r->dz, r->dz64, r->dsint, r->dcost, r->dorient, r->dphi,
                   r->dalpha, r->ddummy, r->dquiet[0], r->dquiet[1]};
   for (void* p : ptrs)
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, s->stream);
   r->buf[0] = r->buf[1] = nullptr;
   r->dx = r->dy = r->dz = r->dsint = r->dcost = r->dorient = r->dphi = nullptr;
   r->dz64 = nullptr;
@@ -235,11 +247,11 @@ static cupf_status admit(cupf_server* s, Request* r, int slot) {
   const int nth = 2 * p.num_theta + 1;
   cudaStream_t st = s->stream;
   auto up = [&](float** d, const std::vector<float>& h) -> cupf_status {
-    CK(cudaMalloc((void**)d, h.size() * sizeof(float)));
+    CK(pool_alloc(s, (void**)d, h.size() * sizeof(float)));
     CK(cudaMemcpyAsync(*d, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, st));
     return CUPF_OK;
   };
-  for (int b = 0; b < 2; ++b) CK(cudaMalloc(&r->buf[b], bb));
+  for (int b = 0; b < 2; ++b) CK(pool_alloc(s, &r->buf[b], bb));
   cupf_status e;
   if ((e = up(&r->dx, r->x)) || (e = up(&r->dy, r->y)) || (e = up(&r->dz, r->z)) ||
       (e = up(&r->dsint, r->sint)) || (e = up(&r->dcost, r->cost)) ||
@@ -248,16 +260,17 @@ static cupf_status admit(cupf_server* s, Request* r, int slot) {
   (void)nth;
   {
     std::vector<double> z64(r->z.begin(), r->z.end());
-    CK(cudaMalloc((void**)&r->dz64, z64.size() * sizeof(double)));
-    CK(cudaMemcpy(r->dz64, z64.data(), z64.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(pool_alloc(s, (void**)&r->dz64, z64.size() * sizeof(double)));
+    CK(cudaMemcpyAsync(r->dz64, z64.data(), z64.size() * sizeof(double), cudaMemcpyHostToDevice,
+                       st));
   }
-  CK(cudaMalloc((void**)&r->dalpha, L * sizeof(int)));
+  CK(pool_alloc(s, (void**)&r->dalpha, L * sizeof(int)));
   CK(cudaMemcpyAsync(r->dalpha, r->alpha.data(), L * sizeof(int), cudaMemcpyHostToDevice, st));
-  CK(cudaMalloc((void**)&r->ddummy, 64 * sizeof(float)));
+  CK(pool_alloc(s, (void**)&r->ddummy, 64 * sizeof(float)));
   CK(cudaMemsetAsync(r->ddummy, 0, 64 * sizeof(float), st));
   const size_t nq = (size_t)r->ntx * r->nty * r->nzc;
   for (int b = 0; b < 2; ++b) {
-    CK(cudaMalloc((void**)&r->dquiet[b], nq));
+    CK(pool_alloc(s, (void**)&r->dquiet[b], nq));
     CK(cudaMemsetAsync(r->dquiet[b], 0, nq, st));
   }
   r->bytes = request_bytes(p, s->pair_bytes, np);
@@ -423,7 +436,7 @@ static cupf_status retire(cupf_server* s, Request* r, int cur) {
   r->res_qoi[0] = v;
   r->res_qoi[1] = a;
   r->res_qoi[2] = v / ((double)(g.fnx - 2) * (g.fny - 2));
-  free_request_device(r);
+  free_request_device(s, r);
   s->used_bytes -= r->bytes;
   s->slots[r->slot] = 0;
   r->slot = -1;
@@ -548,6 +561,16 @@ extern "C" cupf_status cupf_server_create(const cupf_server_config* cfg, cupf_se
   s->pair_bytes = cfg->precision == CUPF_PREC_FP32 ? 8 : 4;
   CK(cudaSetDevice(cfg->device));
   CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  {
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = cfg->device;
+    CK(cudaMemPoolCreate(&s->pool, &props));
+    uint64_t keep = UINT64_MAX;  // hold freed memory for reuse until destroy
+    CK(cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
   CK(cudaEventCreate(&s->ev_round[0]));
   CK(cudaEventCreate(&s->ev_round[1]));
   s->slots.assign(cfg->max_active, 0);
@@ -572,7 +595,9 @@ extern "C" cupf_status cupf_server_destroy(cupf_server* s) {
   if (!s) return cupf_fail(CUPF_ERR_INVALID, "null server");
   cudaSetDevice(s->cfg.device);
   cudaStreamSynchronize(s->stream);
-  for (auto& kv : s->reqs) free_request_device(kv.second.get());
+  for (auto& kv : s->reqs) free_request_device(s, kv.second.get());
+  cudaStreamSynchronize(s->stream);
+  if (s->pool) cudaMemPoolDestroy(s->pool);
   for (cudaEvent_t e : s->ev_round)
     if (e) cudaEventDestroy(e);
   if (s->gexec) cudaGraphExecDestroy(s->gexec);
@@ -667,7 +692,7 @@ extern "C" cupf_status cupf_server_pump(cupf_server* s, int32_t* n_running, int3
     if (slot < 0 || s->used_bytes + need > s->budget) break;
     s->queue.pop_front();
     if ((e = admit(s, r, slot))) {
-      free_request_device(r);
+      free_request_device(s, r);
       r->state = FAILED;
       return e;
     }

@@ -365,7 +365,10 @@ typedef struct cupf_server_config {
   int32_t max_active;       /* resident simulations at most */
   int32_t steps_per_round;  /* steps per graph replay (one pump) */
   int32_t autotune;         /* 1: pick the tile height and z chunk of each grid shape by timing */
-  int64_t hbm_budget_bytes; /* device memory for requests; 0 = free memory - 2 GiB */
+  int64_t hbm_budget_bytes; /* device memory for requests; 0 = free memory - 2 GiB.
+                               Requests' buffers come from a stream-ordered pool that
+                               keeps what retired requests free for later admissions:
+                               up to this much stays held until cupf_server_destroy */
   int32_t tile_y;           /* column-tile height: 0 = the autotuner's pick (8 without
                                autotune), or 4 / 8 for every request */
 } cupf_server_config;
