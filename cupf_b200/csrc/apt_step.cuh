@@ -566,7 +566,8 @@ __device__ __forceinline__ void step_item(const CUtensorMap* tmap, const StepArg
       if (S::kStochastic) return S::make_sr(nv, oid, cell_key * ((uint32_t)(2 * j + 1) * 0x9E3779B9u));
       return S::make(nv, oid);
     };
-    if (RolledSlots<S>::value) {
+    if constexpr (RolledSlots<S>::value) {
+      static_assert(S::kBytes == 4, "the packed id queue holds 16-bit ids");
       // 16-bit pairs: one loop body run to the cell's slot count (the smaller code
       // and register footprint measured faster at three CTAs per SM)
 #pragma unroll
