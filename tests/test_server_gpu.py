@@ -93,3 +93,31 @@ def test_exact_step_targets(built):
         alpha, vols, q = single(ca, n)
         assert r["qoi"] == q, n
         assert np.array_equal(r["alpha"], alpha), n
+
+
+def test_pool_reuse_across_bursts(built):
+    """Retired requests' device memory goes back to the server's pool and serves
+    the next admissions: a second burst of the same requests (in the other order)
+    gives the same results without the server holding more memory, and destroying
+    the server returns what the pool held."""
+    import torch
+    torch.cuda.init()
+    free0, _ = torch.cuda.mem_get_info()
+    ca, cb = req(**A), req(**B)
+    with Server(precision="fp32", steps_per_round=16, autotune=False) as srv:
+        r1 = [srv.submit(ca, 40), srv.submit(cb, 30)]
+        srv.run_until_done(r1)
+        first = [srv.result(r) for r in r1]
+        for r in r1:
+            srv.release(r)
+        free1, _ = torch.cuda.mem_get_info()
+        r2 = [srv.submit(cb, 30), srv.submit(ca, 40)]
+        srv.run_until_done(r2)
+        second = [srv.result(r) for r in r2]
+        free2, _ = torch.cuda.mem_get_info()
+    free3, _ = torch.cuda.mem_get_info()
+    same(first[0], second[1])
+    same(first[1], second[0])
+    assert free1 < free0  # the pool kept the retired requests' memory
+    assert abs(free2 - free1) <= 32 << 20, (free1, free2)
+    assert free3 >= free0 - (64 << 20), (free0, free3)
