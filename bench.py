@@ -351,7 +351,14 @@ def serve_stream(prec, nreq, fix=None, device=0):
         for r in ids:
             srv.release(r)
         # capacity: the same requests all submitted at once (the paced stream
-        # offers about 12 G cell-updates/s, below what one GPU serves)
+        # offers about 12 G cell-updates/s, below what one GPU serves), after an
+        # untimed burst of the same requests for one round each, which leaves the
+        # server's recycled host and device buffers as a server running steadily
+        # holds them
+        warm = [srv.submit(c, 25) for _, c in reqs]
+        srv.run_until_done(warm)
+        for r in warm:
+            srv.release(r)
         busy0, _ = srv.stats()
         with ClockSampler(device) as clk_sat:
             t1 = time.perf_counter()

@@ -60,11 +60,19 @@ namespace {
 
 enum ReqState { PENDING = 0, RUNNING = 1, DONE = 2, FAILED = 3 };
 
+// A page-locked host buffer the server recycles between requests (a request's
+// initial fields and its argmax result): no page faults on refill, and copies
+// to and from the device run at full speed without the driver's staging.
+struct HostBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
 struct Request {
   int64_t id = 0;
   cupf_apt_params p;
-  std::vector<float> x, y, z, sint, cost, orient, phi;
-  std::vector<int> alpha;
+  std::vector<float> x, y, z, sint, cost, orient;
+  HostBuf hphi, halpha;  // initial argmax fields, L values each (until retired)
   int64_t nsteps = 0;
   int state = PENDING;
   double t_submit = 0, t_admit = 0, t_done = 0;
@@ -82,7 +90,8 @@ struct Request {
   size_t bytes = 0;
   int zc = 64, ty = 8, ntx = 0, nty = 0, nzc = 0;
   // results
-  std::vector<int> res_alpha;
+  HostBuf hres;  // argmax grain ids, res_len values
+  size_t res_len = 0;
   std::vector<long long> res_volumes;
   double res_qoi[3] = {0, 0, 0};
 };
@@ -117,6 +126,9 @@ struct cupf_server {
   // server is destroyed), so admitting and retiring cost no device-wide
   // allocation or synchronising free
   cudaMemPool_t pool = nullptr;
+  // recycled page-locked host buffers, at most kHostCacheBytes in all
+  std::vector<HostBuf> host_cache;
+  size_t host_cache_bytes = 0;
   bool dirty = true;
   // (fnx, fny, fnz) -> (tile height, z chunk)
   std::map<std::tuple<int, int, int>, std::pair<int, int>> tile_cache;
@@ -141,6 +153,44 @@ static cupf_status with_fmt(int prec, F&& f) {
 static int gridn(long long n) {
   long long b = (n + 255) / 256;
   return (int)std::max(1ll, std::min(b, 148ll * 16));
+}
+
+constexpr size_t kHostCacheBytes = (size_t)4 << 30;
+
+// A page-locked host buffer of at least n bytes: the smallest cached one that
+// fits, else a new one.
+static cupf_status get_host(cupf_server* s, size_t n, HostBuf* out) {
+  size_t best = s->host_cache.size();
+  for (size_t i = 0; i < s->host_cache.size(); ++i)
+    if (s->host_cache[i].cap >= n &&
+        (best == s->host_cache.size() || s->host_cache[i].cap < s->host_cache[best].cap))
+      best = i;
+  if (best < s->host_cache.size()) {
+    *out = s->host_cache[best];
+    s->host_cache.erase(s->host_cache.begin() + best);
+    s->host_cache_bytes -= out->cap;
+    return CUPF_OK;
+  }
+  out->cap = std::max<size_t>(n, 1);
+  if (cudaHostAlloc(&out->p, out->cap, cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    *out = HostBuf();
+    return cupf_fail(CUPF_ERR_OOM, "page-locked host buffer of %zu bytes", n);
+  }
+  return CUPF_OK;
+}
+
+// Give a host buffer back (no copy may still use it): kept for reuse while the
+// cache stays under its limit, else freed.
+static void put_host(cupf_server* s, HostBuf* b) {
+  if (!b->p) return;
+  if (s->host_cache_bytes + b->cap <= kHostCacheBytes) {
+    s->host_cache.push_back(*b);
+    s->host_cache_bytes += b->cap;
+  } else {
+    cudaFreeHost(b->p);
+  }
+  *b = HostBuf();
 }
 
 // A request's device buffer from the server's pool, ordered on its stream.
@@ -204,7 +254,9 @@ static std::pair<int, int> autotune_tile(cupf_server* s, const Request* r) {
           // single short timing picked different chunks from run to run)
           float ms = 1e30f;
           bool ok = cupf_apt_set_tuning(h, zc) == CUPF_OK &&
-                    cupf_apt_init_from_argmax(h, r->phi.data(), r->alpha.data()) == CUPF_OK &&
+                    cupf_apt_init_from_argmax(h, static_cast<const float*>(r->hphi.p),
+                                              static_cast<const int32_t*>(r->halpha.p)) ==
+                        CUPF_OK &&
                     cupf_apt_step(h, 2, 0) == CUPF_OK;
           for (int rep = 0; ok && rep < 3; ++rep) {
             float m = 0;
@@ -255,8 +307,10 @@ static cupf_status admit(cupf_server* s, Request* r, int slot) {
   cupf_status e;
   if ((e = up(&r->dx, r->x)) || (e = up(&r->dy, r->y)) || (e = up(&r->dz, r->z)) ||
       (e = up(&r->dsint, r->sint)) || (e = up(&r->dcost, r->cost)) ||
-      (e = up(&r->dorient, r->orient)) || (e = up(&r->dphi, r->phi)))
+      (e = up(&r->dorient, r->orient)))
     return e;
+  CK(pool_alloc(s, (void**)&r->dphi, L * sizeof(float)));
+  CK(cudaMemcpyAsync(r->dphi, r->hphi.p, L * sizeof(float), cudaMemcpyHostToDevice, st));
   (void)nth;
   {
     std::vector<double> z64(r->z.begin(), r->z.end());
@@ -265,7 +319,7 @@ static cupf_status admit(cupf_server* s, Request* r, int slot) {
                        st));
   }
   CK(pool_alloc(s, (void**)&r->dalpha, L * sizeof(int)));
-  CK(cudaMemcpyAsync(r->dalpha, r->alpha.data(), L * sizeof(int), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(r->dalpha, r->halpha.p, L * sizeof(int), cudaMemcpyHostToDevice, st));
   CK(pool_alloc(s, (void**)&r->ddummy, 64 * sizeof(float)));
   CK(cudaMemsetAsync(r->ddummy, 0, 64 * sizeof(float), st));
   const size_t nq = (size_t)r->ntx * r->nty * r->nzc;
@@ -418,10 +472,12 @@ static cupf_status retire(cupf_server* s, Request* r, int cur) {
     return CUPF_OK;
   });
   if (e) return e;
-  r->res_alpha.resize(L);
+  cupf_status he = get_host(s, L * sizeof(int), &r->hres);
+  if (he) return he;
+  r->res_len = L;
   std::vector<unsigned long long> c(ng + 1);
   std::vector<double> part(2 * nb);
-  CK(cudaMemcpyAsync(r->res_alpha.data(), r->dalpha, L * sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(r->hres.p, r->dalpha, L * sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(c.data(), s->d_counts, c.size() * sizeof(unsigned long long),
                      cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(part.data(), s->d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost,
@@ -443,8 +499,9 @@ static cupf_status retire(cupf_server* s, Request* r, int cur) {
   r->state = DONE;
   r->t_done = now_s();
   r->x.clear();
-  r->phi.clear();
-  r->alpha.clear();
+  // the uploads of the initial fields finished long ago (the stream was waited on)
+  put_host(s, &r->hphi);
+  put_host(s, &r->halpha);
   s->dirty = true;
   return CUPF_OK;
 }
@@ -598,6 +655,10 @@ extern "C" cupf_status cupf_server_destroy(cupf_server* s) {
   for (auto& kv : s->reqs) free_request_device(s, kv.second.get());
   cudaStreamSynchronize(s->stream);
   if (s->pool) cudaMemPoolDestroy(s->pool);
+  for (auto& kv : s->reqs)
+    for (HostBuf* b : {&kv.second->hphi, &kv.second->halpha, &kv.second->hres})
+      if (b->p) cudaFreeHost(b->p);
+  for (HostBuf& b : s->host_cache) cudaFreeHost(b.p);
   for (cudaEvent_t e : s->ev_round)
     if (e) cudaEventDestroy(e);
   if (s->gexec) cudaGraphExecDestroy(s->gexec);
@@ -644,8 +705,14 @@ extern "C" cupf_status cupf_server_submit(cupf_server* s, const cupf_apt_params*
   r->orient.resize(4 * (size_t)(p->num_theta + 1));
   pack_orientations(in->sint, in->cost, p->num_theta, r->orient.data());
   const size_t L = (size_t)p->fnx * p->fny * p->fnz;
-  r->phi.assign(phi, phi + L);
-  r->alpha.assign(alpha, alpha + L);
+  cupf_status e;
+  if ((e = get_host(s, L * sizeof(float), &r->hphi))) return e;
+  if ((e = get_host(s, L * sizeof(int32_t), &r->halpha))) {
+    put_host(s, &r->hphi);
+    return e;
+  }
+  std::memcpy(r->hphi.p, phi, L * sizeof(float));
+  std::memcpy(r->halpha.p, alpha, L * sizeof(int32_t));
   r->nsteps = nsteps;
   r->t_submit = now_s();
   *request_id = r->id;
@@ -729,7 +796,7 @@ extern "C" cupf_status cupf_server_result(cupf_server* s, int64_t id, int32_t* s
   Request* r = it->second.get();
   *status = r->state;
   if (r->state != DONE) return CUPF_OK;
-  if (alpha_out) std::memcpy(alpha_out, r->res_alpha.data(), r->res_alpha.size() * sizeof(int));
+  if (alpha_out && r->hres.p) std::memcpy(alpha_out, r->hres.p, r->res_len * sizeof(int));
   if (volumes_out) {
     const int n = std::min<int>(num_grains + 1, (int)r->res_volumes.size());
     for (int i = 0; i < n; ++i) volumes_out[i] = r->res_volumes[i];
@@ -780,6 +847,12 @@ extern "C" cupf_status cupf_server_release(cupf_server* s, int64_t id) {
     auto q = std::find(s->queue.begin(), s->queue.end(), id);
     if (q != s->queue.end()) s->queue.erase(q);
   }
+  Request* r = it->second.get();
+  // a request that failed during admission may still have an upload queued
+  if (r->state == FAILED) CK(cudaStreamSynchronize(s->stream));
+  put_host(s, &r->hphi);
+  put_host(s, &r->halpha);
+  put_host(s, &r->hres);
   s->reqs.erase(it);
   return CUPF_OK;
 }
