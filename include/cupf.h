@@ -377,8 +377,10 @@ cupf_status cupf_server_create(const cupf_server_config* cfg, cupf_server** out)
 cupf_status cupf_server_destroy(cupf_server* s);
 
 /* Queue a simulation: parameters and inputs as for cupf_apt_create, initial
- * argmax fields as for cupf_apt_init_from_argmax (all copied), nsteps explicit
- * steps (line / cylinder thermal types).  *request_id identifies it. */
+ * argmax fields as for cupf_apt_init_from_argmax (all copied, the fields into
+ * page-locked host buffers the server recycles between requests, up to 4 GiB),
+ * nsteps explicit steps (line / cylinder thermal types).  *request_id
+ * identifies it. */
 cupf_status cupf_server_submit(cupf_server* s, const cupf_apt_params* p,
                                const cupf_apt_inputs* in, const float* phi,
                                const int32_t* alpha, int64_t nsteps, int64_t* request_id);
