@@ -144,3 +144,25 @@ def test_qoi_sums_match_fp64_numpy(built, prec):
     # same FP64 formulas over the same values; only the summation order differs
     for got, want in zip(q, ref):
         assert abs(got - want) <= 1e-12 * max(1.0, abs(want)), (q, ref)
+
+
+def test_collect_into_caller_arrays(built):
+    """collect(out=...) reads the argmax fields into caller-owned arrays (here
+    page-locked ones) with the same values as the default path, and rejects
+    arrays of the wrong type or length."""
+    import torch
+    c = cases.line_case(40, 36, 48, num_pf=5, num_grains=20, seed=4, bc="110")
+    out = (torch.empty(c.length, dtype=torch.float32, pin_memory=True).numpy(),
+           torch.empty(c.length, dtype=torch.int32, pin_memory=True).numpy())
+    with APTSolver(c) as s:
+        s.init_from_argmax(c.phi, c.alpha)
+        s.step(20)
+        phi0, alpha0 = s.collect(clear=True)
+        phi1, alpha1 = s.collect(clear=True, out=out)
+        with pytest.raises(ValueError):
+            s.collect(out=(np.empty(c.length, np.float64), out[1]))
+        with pytest.raises(ValueError):
+            s.collect(out=(out[0][:-1], out[1]))
+    assert phi1 is out[0] and alpha1 is out[1]
+    assert np.array_equal(phi0.view(np.uint32), phi1.view(np.uint32))
+    assert np.array_equal(alpha0, alpha1)
